@@ -1,0 +1,353 @@
+"""Benchmark: fused far-field forward + loss + adjoint throughput (patterns/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1] [--no-cpu-baseline]
+
+Workload (default ``c1``): 1536^2 complex64 object, 128^2 probe, 40 x 40 raster
+(1600 positions, 32 px step, U[-3,3] jitter), Poisson loss at a 1e4-photon
+peak, batch 256 patterns per GPU, seeded synthetic data (the reference's
+datasets are not distributed).  One step = one minibatch: the fused
+forward/loss/adjoint kernel plus the deterministic dO/dP assembly (and, for
+N > 1, the NCCL all-reduce of dO and dP -- each rank handles its own
+minibatch, so per-GPU work is fixed: weak scaling).  L2 is flushed (a 256 MiB
+write) before every timed step; step times are CUDA events on the launching
+stream, summed over K steps, max over ranks.
+
+``--impl reference`` times the reference's own torch CPU path (per-frame
+loop of Recovery.py:288-316 with autograd) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "conventional-ptychography-reconstruction_b200"
+
+METRIC = "fwd+adj patterns/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def algorithmic_bytes_per_pattern(M: int, B: int) -> float:
+    """Object window read (8 M^2) + measurement read (4 M^2) + object-gradient
+    contribution write (8 M^2), plus probe read and probe-gradient write
+    amortised over the batch (16 M^2 / B)."""
+    return 20.0 * M * M + 16.0 * M * M / B
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(kernel_key: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def cpu_reference_rate(work, batch: int, budget_s: float, threads: int | None = None):
+    """Time the reference's torch CPU path on a bounded sample (whole minibatches)."""
+    from oracle import torch_cpu_path
+    if threads:
+        torch.set_num_threads(threads)
+    M = work["probe"].shape[0]
+    obj = torch.from_numpy(work["obj"].astype(np.complex64)).requires_grad_(True)
+    probe = torch.from_numpy(work["probe"].astype(np.complex64)).requires_grad_(True)
+    stack = torch.from_numpy(np.ascontiguousarray(np.moveaxis(work["Imeas"], 0, -1)))  # [M, M, F]
+    F = stack.shape[2]
+    rng = np.random.default_rng(5)
+    n, t_total, steps = 0, 0.0, 0
+    lt = work["workload"].loss_type
+    while t_total < budget_s or steps == 0:
+        idx = rng.permutation(F)[:batch]
+        t0 = time.perf_counter()
+        torch_cpu_path.minibatch_fwd_adj(obj, probe, work["tlY"], work["tlX"], stack, idx, lt)
+        t_total += time.perf_counter() - t0
+        n += len(idx)
+        steps += 1
+    return n / t_total, n, steps, torch.get_num_threads()
+
+
+def run_reference(args):
+    """--impl reference: the reference's torch CPU path on this host's cores."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pkg = importlib.import_module(PKG)
+    work = pkg.synth.make_workload(args.workload, device=None)
+    w = work["workload"]
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    from oracle import torch_cpu_path
+    M = w.probe
+    obj = torch.from_numpy(work["obj"].astype(np.complex64)).requires_grad_(True)
+    probe = torch.from_numpy(work["probe"].astype(np.complex64)).requires_grad_(True)
+    stack = torch.from_numpy(np.ascontiguousarray(np.moveaxis(work["Imeas"], 0, -1)))
+    F = stack.shape[2]
+    rng = np.random.default_rng(5)
+    batch = args.ref_batch or w.batch
+    for _ in range(args.warmup):
+        torch_cpu_path.minibatch_fwd_adj(obj, probe, work["tlY"], work["tlX"], stack,
+                                         rng.permutation(F)[:batch], w.loss_type)
+    t = 0.0
+    for _ in range(args.steps):
+        idx = rng.permutation(F)[:batch]
+        t0 = time.perf_counter()
+        torch_cpu_path.minibatch_fwd_adj(obj, probe, work["tlY"], work["tlX"], stack, idx, w.loss_type)
+        t += time.perf_counter() - t0
+    rate = batch * args.steps / t
+    sample = (f"{args.steps} minibatches of {batch} of the {F} patterns (per-frame torch CPU loop "
+              f"+ autograd, reference restatement)")
+    line = {"metric": METRIC, "value": rate, "unit": "patterns/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (fp32)",
+            "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": _config(w, batch, args),
+            "cpu_baseline": {"value": rate, "unit": "patterns/s", "cores": torch.get_num_threads(),
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": "patterns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _config(w, batch, args):
+    return {"workload": w.name, "canvas": w.canvas, "probe": w.probe, "positions": w.n_scan ** 2,
+            "batch_per_gpu": batch, "loss": w.loss_type, "peak_photons": w.peak,
+            "l2": "flushed before every timed step (256 MiB write)"}
+
+
+def run_ours(args):
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    pkg = importlib.import_module(PKG)
+    work = pkg.synth.make_workload(args.workload, device=dev)
+    w = work["workload"]
+    M, B = w.probe, w.batch
+    O = torch.from_numpy(work["obj"].astype(np.complex64)).to(dev)
+    P = torch.from_numpy(work["probe"].astype(np.complex64)).to(dev)
+    tl = pkg.make_windows(work["tlY"], work["tlX"], dev)
+    pkg.check_windows(tl, O.shape, M)
+    stack = torch.from_numpy(work["Imeas"]).to(dev)  # [F, M, M], resident
+    F = stack.shape[0]
+    H, W = O.shape
+    # each rank draws its own minibatches (seeded per rank)
+    g = torch.Generator().manual_seed(1234 + rank)
+    nb = args.warmup + args.steps
+    batches = [torch.randperm(F, generator=g)[:B].to(torch.int32).to(dev) for _ in range(nb)]
+    dO = torch.empty((H, W), dtype=torch.complex64, device=dev)
+    dP = torch.empty((M, M), dtype=torch.complex64, device=dev)
+    ws = pkg.optics.FwdAdjWorkspace()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    code = pkg.LOSS_CODES[w.loss_type]
+    s = torch.cuda.current_stream(dev)
+
+    def step(i):
+        loss, _, _, _ = pkg.fwd_adj_raw(O, P, tl, stack, code, batch=batches[i], dO=dO, dP=dP, workspace=ws)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(torch.view_as_real(dO))
+            dist.all_reduce(torch.view_as_real(dP))
+        return loss
+
+    for i in range(args.warmup):
+        step(i)
+        flush.zero_()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(s)
+            step(args.warmup + k)
+            ev[k][1].record(s)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = [a.elapsed_time(b) for a, b in ev]  # ms
+    t_tot = torch.tensor([sum(times)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_tot, op=dist.ReduceOp.MAX)
+    t_max_ms = float(t_tot)
+    value = world * B * args.steps / (t_max_ms / 1e3)
+    launches = 5 * args.steps  # k_fused, k_bin, k_dO, k_dP_part, k_dP_final per step
+
+    # ---- e2e: public API, host-pinned inputs copied in every step -------------
+    e2e = None
+    if True:
+        Im_host = [stack.index_select(0, batches[i].long()).cpu().pin_memory() for i in range(min(nb, 4))]
+        tl_host = [tl.index_select(0, batches[i].long()).cpu().pin_memory() for i in range(min(nb, 4))]
+        Oparam = O.clone().requires_grad_(True)
+        Pparam = P.clone().requires_grad_(True)
+        out_host = torch.empty((), dtype=torch.float64).pin_memory()
+
+        def e2e_step(i):
+            Im_d = Im_host[i % len(Im_host)].to(dev, non_blocking=True)
+            tl_d = tl_host[i % len(tl_host)].to(dev, non_blocking=True)
+            Oparam.grad = None
+            Pparam.grad = None
+            loss = pkg.fused_loss(Oparam, Pparam, tl_d, Im_d, w.loss_type)
+            loss.backward()
+            out_host.copy_(loss.detach(), non_blocking=True)
+
+        for i in range(args.warmup):
+            e2e_step(i)
+        torch.cuda.synchronize()
+        e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            e_ev[k][0].record(s)
+            e2e_step(k)
+            e_ev[k][1].record(s)
+        torch.cuda.synchronize()
+        et = torch.tensor([sum(a.elapsed_time(b) for a, b in e_ev)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * B * args.steps / (float(et) / 1e3), "unit": "patterns/s",
+               "h2d_bytes_per_step": int(Im_host[0].numel() * 4 + tl_host[0].numel() * 4),
+               "d2h_bytes_per_step": 8,
+               "note": "fused_loss + backward through the public API; measurements and windows "
+                       "copied from pinned host memory every step"}
+
+    if rank == 0:
+        peak, kind = measured_peak_hbm()
+        bpp = algorithmic_bytes_per_pattern(M, B)
+        step_s = (t_max_ms / 1e3) / args.steps
+        achieved = bpp * B / step_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": f"of {kind}",
+                "kernel": "ptycho_fwd_adj (k_fused + gradient assembly), per call of one minibatch",
+                "algorithmic_bytes_per_pattern": bpp, "traffic": load_traffic(f"{args.workload}_fwd_adj")}
+        line = {"metric": METRIC, "value": value, "unit": "patterns/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (fp32), fp64 loss reduction",
+                "data": "synthetic (seeded generator; reference datasets not distributed)",
+                "config": _config(w, B, args), "roofline": roof, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        if not args.no_cpu_baseline and world == 1:
+            rate, n, steps, cores = cpu_reference_rate(work, B, budget_s=args.cpu_budget)
+            line["cpu_baseline"] = {"value": rate, "unit": "patterns/s", "cores": cores, "kind": "port",
+                                    "sample": f"{steps} minibatches x {B} patterns ({n} patterns) of the "
+                                              f"same workload, per-frame torch CPU loop + autograd "
+                                              f"(reference restatement), {cores} threads"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-batch", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,71 @@
+"""ctypes binding of the C ABI in ``include/ptycho_b200.h``.
+
+The shared library ``libptycho_b200.so`` is built in-tree by ``csrc/build.py``.
+There is no fallback: if the library is missing or a call fails, a
+``RuntimeError`` is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libptycho_b200.so")
+
+_c_int, _c_size, _vp = ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p
+_c_uint, _c_float, _c_double = ctypes.c_uint, ctypes.c_float, ctypes.c_double
+
+# name -> (restype, argtypes); every entry is declared in include/ptycho_b200.h
+SIGNATURES = {
+    "ptycho_status_string": (ctypes.c_char_p, [_c_int]),
+    "ptycho_version": (_c_int, []),
+    "ptycho_forward_intensity": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp,
+                                          _c_int, _vp, _vp, _vp]),
+    "ptycho_fwd_adj_workspace_size": (_c_size, [_c_int, _c_int, _c_int, _c_int, _c_int]),
+    "ptycho_fwd_adj": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _c_int,
+                                _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _c_size, _vp, _vp]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load (once) and return the library with all signatures declared."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with "
+                    "`python conventional-ptychography-reconstruction_b200/csrc/build.py` "
+                    "(or __graft_entry__.build()); there is no CPU fallback")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+class PtychoError(RuntimeError):
+    """A non-zero ptycho_status returned by the library."""
+
+    def __init__(self, code: int, where: str):
+        msg = lib().ptycho_status_string(code).decode()
+        super().__init__(f"{where}: {msg} (status {code})")
+        self.code = code
+
+
+def check(code: int, where: str) -> None:
+    if code != 0:
+        raise PtychoError(code, where)
+
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported size", 3: "misaligned pointer",
+          4: "workspace too small", 5: "CUDA launch failed", 6: "scan window outside the canvas",
+          7: "bounded wait timed out"}

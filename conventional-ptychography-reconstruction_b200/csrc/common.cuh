@@ -1,0 +1,30 @@
+// common.cuh -- shared device helpers for the ptychography kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ptycho_b200.h"
+
+#define PTY_DEVI __device__ __forceinline__
+
+PTY_DEVI float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+PTY_DEVI float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+PTY_DEVI float2 c_mul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+PTY_DEVI float2 c_mulc(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+PTY_DEVI float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+PTY_DEVI float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// Record an error code in a device status word (first writer wins; never cleared).
+PTY_DEVI void pty_raise(int32_t* status, int code) {
+  if (status) atomicCAS(reinterpret_cast<int*>(status), 0, code);
+}
+
+static inline bool pty_aligned(const void* p, size_t a) {
+  return (reinterpret_cast<uintptr_t>(p) % a) == 0;
+}
+static inline size_t pty_align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }

@@ -1,0 +1,287 @@
+"""Forward model, losses and adjoint on the B200 kernels (drop-in for the
+reference's ``utils/optics.py`` forward path and the per-frame loop of
+``Recovery.py:288-316``).
+
+Public functions:
+
+* :func:`scan_positions_to_pixels` -- utils/optics.py:68-99, same signature
+  and outputs (host NumPy, bit-exact with the reference);
+* :func:`forward_imaging_model` -- utils/optics.py:102-112, same signature,
+  differentiable w.r.t. object and probe;
+* :func:`forward_intensity` -- the batched form: ``I[b] = |fftshift(fft2(P *
+  O[window_b]))|^2`` for a stack of windows;
+* :func:`fused_loss` -- the fused forward + loss + adjoint used by the
+  training loop: returns the FP64 sum over the batch of per-pattern mean
+  losses (Recovery.py:294-307) as a differentiable scalar whose backward
+  returns the gradients computed in the same kernel pass.
+
+All compute runs in ``libptycho_b200.so``; there is no CPU path.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+
+LOSS_CODES = {"smooth_L1_loss": 0, "FD_loss": 1, "Poisson_likelihood_loss": 2}
+_INTENSITY_GRAD = 3
+SUPPORTED_PROBE_SIZES = (64, 128)
+
+
+# --------------------------------------------------------------------------
+# geometry (host) -- utils/optics.py:68-99
+# --------------------------------------------------------------------------
+def scan_positions_to_pixels(xlocation, ylocation, probe_shape, wavelength, camera_length,
+                             camera_pixel_pitch):
+    """Physical scan positions (metres) -> sample-plane pixel windows.
+
+    Same contract as utils/optics.py:68-99: returns ``(tlX, tlY, brX, brY, dx,
+    canvas_size)``; indices use NumPy's round-half-to-even of ``pos / dx``
+    with ``dx = wavelength * camera_length / ([M, N] * camera_pixel_pitch)``;
+    the canvas is the larger bottom-right extent rounded up to a multiple of 6.
+    """
+    M, N = probe_shape
+    x_pos = np.asarray(xlocation).squeeze() - np.min(xlocation)
+    y_pos = np.asarray(ylocation).squeeze() - np.min(ylocation)
+    dx = wavelength * camera_length / (np.array([M, N]) * camera_pixel_pitch)
+    tlY = np.round(y_pos / dx[0]).astype(int)
+    tlX = np.round(x_pos / dx[1]).astype(int)
+    brY = tlY + M
+    brX = tlX + N
+    max_size = max(int(np.max(brY)), int(np.max(brX)))
+    canvas_size = math.ceil(max_size / 6) * 6
+    return tlX, tlY, brX, brY, dx, canvas_size
+
+
+def make_windows(tlY, tlX, device=None) -> torch.Tensor:
+    """Pack top-left corners into the library's [B, 2] int32 (tlY, tlX) layout."""
+    tlY = torch.as_tensor(np.asarray(tlY), dtype=torch.int32).reshape(-1)
+    tlX = torch.as_tensor(np.asarray(tlX), dtype=torch.int32).reshape(-1)
+    t = torch.stack([tlY, tlX], dim=1).contiguous()
+    return t.to(device) if device is not None else t
+
+
+def check_windows(tl: torch.Tensor, canvas_hw, M: int) -> None:
+    """Host-side bounds check of scan windows (raises ``ValueError``)."""
+    H, W = canvas_hw
+    t = tl.detach().to("cpu")
+    if t.numel() == 0:
+        return
+    bad = (t[:, 0] < 0) | (t[:, 1] < 0) | (t[:, 0] > H - M) | (t[:, 1] > W - M)
+    if bool(bad.any()):
+        i = int(torch.nonzero(bad)[0, 0])
+        raise ValueError(f"scan window {i} at {t[i].tolist()} leaves the {H}x{W} canvas (probe {M})")
+
+
+# --------------------------------------------------------------------------
+# raw calls
+# --------------------------------------------------------------------------
+def _stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _as_c64(x: torch.Tensor, name: str) -> torch.Tensor:
+    if not x.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (there is no CPU path)")
+    if x.dtype != torch.complex64:
+        x = x.to(torch.complex64)
+    return x.contiguous()
+
+
+def _check_probe(P: torch.Tensor) -> int:
+    if P.dim() != 2 or P.shape[0] != P.shape[1] or P.shape[0] not in SUPPORTED_PROBE_SIZES:
+        raise ValueError(f"probe must be square with size in {SUPPORTED_PROBE_SIZES}, got "
+                         f"{tuple(P.shape)}")
+    return int(P.shape[0])
+
+
+_status_cache: dict = {}
+
+
+def device_status(device) -> torch.Tensor:
+    """The per-device int32 status word the kernels raise errors into."""
+    device = torch.device(device)
+    st = _status_cache.get(device)
+    if st is None:
+        st = torch.zeros(1, dtype=torch.int32, device=device)
+        _status_cache[device] = st
+    return st
+
+
+def read_status(device, reset: bool = True) -> int:
+    """Synchronously read (and optionally clear) the device status word."""
+    st = device_status(device)
+    v = int(st.item())
+    if reset:
+        st.zero_()
+    return v
+
+
+def _batch_arg(batch, dev):
+    if batch is None:
+        return None
+    return torch.as_tensor(batch).to(device=dev, dtype=torch.int32).contiguous()
+
+
+def forward_intensity(O: torch.Tensor, P: torch.Tensor, tl: torch.Tensor, batch=None) -> torch.Tensor:
+    """Far-field intensities ``[B, M, M]`` float32 (no autograd).
+
+    ``tl`` [F, 2] int32 windows of all frames; ``batch`` [B] frame ids (None:
+    all F frames in order)."""
+    O = _as_c64(O, "object")
+    P = _as_c64(P, "probe")
+    M = _check_probe(P)
+    H, W = O.shape
+    tl = tl.to(device=O.device, dtype=torch.int32).contiguous()
+    F = int(tl.shape[0])
+    bt = _batch_arg(batch, O.device)
+    B = F if bt is None else int(bt.numel())
+    out = torch.empty((B, M, M), dtype=torch.float32, device=O.device)
+    st = device_status(O.device)
+    _lib.check(_lib.lib().ptycho_forward_intensity(
+        O.data_ptr(), H, W, P.data_ptr(), M, M, tl.data_ptr(), F,
+        bt.data_ptr() if bt is not None else None, B, out.data_ptr(), st.data_ptr(),
+        _stream_handle(O.device)), "ptycho_forward_intensity")
+    return out
+
+
+class FwdAdjWorkspace:
+    """Reusable device scratch for ``ptycho_fwd_adj`` (grows on demand)."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, nbytes: int, device) -> torch.Tensor:
+        nbytes = max(int(nbytes), 256)
+        if self.buf is None or self.buf.numel() < nbytes or self.buf.device != torch.device(device):
+            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        return self.buf
+
+
+_default_ws: dict = {}
+
+
+def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = True,
+                per_pattern: bool = False, dO=None, dP=None, accumulate: bool = False,
+                workspace: "FwdAdjWorkspace | None" = None):
+    """One call of ``ptycho_fwd_adj``.  Returns ``(loss_total, loss_per_pattern|None, dO, dP)``.
+
+    ``tl`` [F, 2] int32 and ``Imeas`` [F, M, M] float32 describe all frames;
+    ``batch`` [B] selects the frames of this call (None: all, in order).
+    ``loss_total`` is a 0-d float64 CUDA tensor.  Gradient buffers are
+    allocated unless given (``accumulate`` adds into given buffers)."""
+    O = _as_c64(O, "object")
+    P = _as_c64(P, "probe")
+    M = _check_probe(P)
+    H, W = O.shape
+    dev = O.device
+    tl = tl.to(device=dev, dtype=torch.int32).contiguous()
+    F = int(tl.shape[0])
+    if Imeas.dtype != torch.float32 or not Imeas.is_contiguous() or Imeas.device != dev:
+        Imeas = Imeas.to(device=dev, dtype=torch.float32).contiguous()
+    if Imeas.shape != (F, M, M):
+        raise ValueError(f"measurements must be [F, M, M] = {(F, M, M)}, got {tuple(Imeas.shape)}")
+    bt = _batch_arg(batch, dev)
+    B = F if bt is None else int(bt.numel())
+    loss_total = torch.empty((), dtype=torch.float64, device=dev)
+    lp = torch.empty(B, dtype=torch.float64, device=dev) if per_pattern else None
+    if want_grad:
+        if dO is None:
+            dO = torch.empty((H, W), dtype=torch.complex64, device=dev)
+        if dP is None:
+            dP = torch.empty((M, M), dtype=torch.complex64, device=dev)
+    else:
+        dO = dP = None
+    ws_bytes = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, M, B))
+    if workspace is None:
+        workspace = _default_ws.setdefault(dev, FwdAdjWorkspace())
+    ws = workspace.get(ws_bytes, dev)
+    st = device_status(dev)
+    _lib.check(_lib.lib().ptycho_fwd_adj(
+        O.data_ptr(), H, W, P.data_ptr(), M, M, tl.data_ptr(), Imeas.data_ptr(), F,
+        bt.data_ptr() if bt is not None else None, B, int(loss_code),
+        lp.data_ptr() if lp is not None else None, loss_total.data_ptr(),
+        dO.data_ptr() if dO is not None else None, dP.data_ptr() if dP is not None else None,
+        1 if accumulate else 0, ws.data_ptr(), ws.numel(), st.data_ptr(),
+        _stream_handle(dev)), "ptycho_fwd_adj")
+    return loss_total, lp, dO, dP
+
+
+# --------------------------------------------------------------------------
+# autograd
+# --------------------------------------------------------------------------
+class _FusedLoss(torch.autograd.Function):
+    """Loss of a batch with the adjoint fused into the same kernel pass.
+
+    forward: one ``ptycho_fwd_adj`` call computes the FP64 loss and, when any
+    input needs a gradient, dO and dP; backward scales them by the incoming
+    gradient (exit waves are never stored)."""
+
+    @staticmethod
+    def forward(ctx, O, P, tl, Imeas, loss_code, batch):
+        need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1]
+        loss, _, dO, dP = fwd_adj_raw(O, P, tl, Imeas, loss_code, batch=batch, want_grad=need)
+        if need:
+            ctx.save_for_backward(dO, dP)
+        ctx.need = need
+        return loss
+
+    @staticmethod
+    def backward(ctx, g):
+        if not ctx.need:
+            return None, None, None, None, None, None
+        dO, dP = ctx.saved_tensors
+        s = g.to(torch.float32)
+        gO = dO * s if ctx.needs_input_grad[0] else None
+        gP = dP * s if ctx.needs_input_grad[1] else None
+        return gO, gP, None, None, None, None
+
+
+def fused_loss(object_complex: torch.Tensor, probe_complex: torch.Tensor, tl: torch.Tensor,
+               Imeas: torch.Tensor, loss_type: str = "smooth_L1_loss", batch=None) -> torch.Tensor:
+    """Sum over the batch of the per-pattern mean loss (Recovery.py:288-307).
+
+    ``tl`` [F, 2] int32 (tlY, tlX) and ``Imeas`` [F, M, M] float32 for all
+    frames; ``batch`` [B] frame ids of this minibatch (None: all frames).
+    Returns a 0-d float64 tensor; ``backward()`` deposits dO / dP (torch's
+    complex convention) into the inputs that require grad."""
+    if loss_type not in LOSS_CODES:
+        raise ValueError(f"loss_type must be one of {tuple(LOSS_CODES)}, got {loss_type!r}")
+    if object_complex.dtype != torch.complex64 or probe_complex.dtype != torch.complex64:
+        raise TypeError("object and probe must be complex64")
+    return _FusedLoss.apply(object_complex, probe_complex, tl, Imeas, LOSS_CODES[loss_type], batch)
+
+
+class _ForwardIntensity(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, O, P, tl):
+        ctx.save_for_backward(O, P, tl)
+        return forward_intensity(O, P, tl)
+
+    @staticmethod
+    def backward(ctx, gI):
+        O, P, tl = ctx.saved_tensors
+        _, _, dO, dP = fwd_adj_raw(O.detach(), P.detach(), tl, gI.contiguous(), _INTENSITY_GRAD)
+        return (dO if ctx.needs_input_grad[0] else None,
+                dP if ctx.needs_input_grad[1] else None, None)
+
+
+def forward_intensity_batched(O: torch.Tensor, P: torch.Tensor, tl: torch.Tensor) -> torch.Tensor:
+    """Differentiable batched intensities [B, M, M] (backward through the adjoint kernel)."""
+    return _ForwardIntensity.apply(O, P, tl)
+
+
+def forward_imaging_model(object_complex, probe_complex, tlY, tlX, brY, brX):
+    """Drop-in for utils/optics.py:102-112: ``|fftshift(fft2(P * O[tlY:brY, tlX:brX]))|^2``.
+
+    Scalar window corners as in the reference; differentiable."""
+    M = int(brY) - int(tlY)
+    N = int(brX) - int(tlX)
+    if (M, N) != tuple(probe_complex.shape):
+        raise ValueError(f"window {(M, N)} does not match probe {tuple(probe_complex.shape)}")
+    tl = torch.tensor([[int(tlY), int(tlX)]], dtype=torch.int32, device=object_complex.device)
+    check_windows(tl, object_complex.shape, M)
+    return forward_intensity_batched(object_complex, probe_complex, tl)[0]

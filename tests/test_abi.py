@@ -1,0 +1,74 @@
+"""The C-ABI library loads without a GPU and exports every declared symbol;
+argument validation that happens before any device work returns the
+documented status codes."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, load_pkg
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(ptycho_\w+)\s*\(", src):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    pkg = load_pkg()
+    L = pkg.lib()
+    declared = _declared_symbols()
+    assert declared, "no declarations found"
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, missing
+    # the ctypes signature table covers exactly the declared functions
+    assert set(pkg._lib.SIGNATURES) == declared
+
+
+def test_status_strings_and_version():
+    L = load_pkg().lib()
+    assert L.ptycho_version() >= 100
+    for code, text in load_pkg()._lib.STATUS.items():
+        assert L.ptycho_status_string(code).decode() == text
+
+
+def test_validation_before_device_work():
+    L = load_pkg().lib()
+    fake = ctypes.c_void_p(4096)  # never dereferenced: validation fails first
+    # unsupported probe size
+    assert L.ptycho_fwd_adj(fake, 256, 256, fake, 32, 32, fake, fake, 4, None, 4, 0, None, None, None,
+                            None, 0, fake, 1 << 30, None, None) == 2
+    # non-square probe
+    assert L.ptycho_forward_intensity(fake, 256, 256, fake, 64, 128, fake, 1, None, 1, fake, None,
+                                      None) == 2
+    # null object
+    assert L.ptycho_forward_intensity(None, 256, 256, fake, 64, 64, fake, 1, None, 1, fake, None,
+                                      None) == 1
+    # batch larger than the frame count without explicit frame ids
+    assert L.ptycho_forward_intensity(fake, 256, 256, fake, 64, 64, fake, 1, None, 2, fake, None,
+                                      None) == 1
+    # bad loss type
+    assert L.ptycho_fwd_adj(fake, 256, 256, fake, 64, 64, fake, fake, 4, None, 4, 9, None, None, None,
+                            None, 0, fake, 1 << 30, None, None) == 1
+    # workspace too small
+    assert L.ptycho_fwd_adj(fake, 256, 256, fake, 64, 64, fake, fake, 4, None, 4, 0, None, None, None,
+                            None, 0, fake, 16, None, None) == 4
+    # misaligned object pointer
+    assert L.ptycho_forward_intensity(ctypes.c_void_p(4097), 256, 256, fake, 64, 64, fake, 1, None, 1,
+                                      fake, None, None) == 3
+
+
+def test_workspace_size_monotone():
+    L = load_pkg().lib()
+    a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)
+    b = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 512)
+    assert 0 < a < b
+    assert a >= 256 * 128 * 128 * 8
+    assert L.ptycho_fwd_adj_workspace_size(-1, 5, 64, 64, 1) == 0
