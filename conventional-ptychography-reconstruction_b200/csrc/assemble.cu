@@ -1,0 +1,184 @@
+// assemble.cu -- deterministic assembly of object and probe gradients.
+//
+// Replaces the accumulation that torch autograd performs for
+// `probe * object[tlY:brY, tlX:brX]` (Recovery.py:290, backward at :316):
+//   dO[window_b] += G_b * conj(P),   dP += G_b * conj(O[window_b]),
+// with G_b = dL/dpsi_b = (-1)^(x+y) E'_b (E'_b written by the fused kernel).
+// No floating-point atomics: every output element is owned by one thread
+// that sums its contributions in ascending pattern order; the dP group
+// partials are summed in group order by whichever block arrives last (an
+// integer arrival counter picks it, the order of the sum does not depend on it).
+#include "assemble.cuh"
+
+namespace pty {
+
+PTY_DEVI float2 c_negif(float2 a, int odd) { return odd ? make_float2(-a.x, -a.y) : a; }
+
+// dO over one kTile x kTile canvas tile, 256 threads x kTile/8 rows.
+__global__ void __launch_bounds__(256) k_dO(const float2* __restrict__ Eb, const float2* __restrict__ P,
+                                            const int2* __restrict__ tlb, int B, int H, int W, int M,
+                                            int ntx, float2* __restrict__ dO, int accumulate) {
+  __shared__ int list[256];
+  __shared__ int wcnt[8];
+  const int tile = blockIdx.x;
+  const int ty0 = (tile / ntx) * kTile, tx0 = (tile % ntx) * kTile;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int X = tx0 + lane;
+  const int Y0 = ty0 + w;
+  constexpr int R = kTile / 8;
+  float2 acc[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) acc[j] = make_float2(0.f, 0.f);
+  for (int b0 = 0; b0 < B; b0 += 256) {
+    const int b = b0 + threadIdx.x;
+    bool hit = false;
+    if (b < B) {
+      const int2 c = __ldg(tlb + b);
+      hit = c.x >= 0 && c.x < ty0 + kTile && c.x + M > ty0 && c.y < tx0 + kTile && c.y + M > tx0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) wcnt[w] = __popc(m);
+    __syncthreads();
+    int off = 0, n = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      off += i < w ? wcnt[i] : 0;
+      n += wcnt[i];
+    }
+    if (hit) list[off + __popc(m & ((1u << lane) - 1u))] = b;
+    __syncthreads();
+    // two patterns per iteration: loads first, then the adds in list order
+    for (int i = 0; i < n; i += 2) {
+      float2 c0[R], c1[R];
+      {
+        const int bb = list[i];
+        const int2 c = __ldg(tlb + bb);
+        const int lx = X - c.y;
+        const float2* Ep = Eb + size_t(bb) * M * M;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int ly = Y0 + 8 * j - c.x;
+          c0[j] = make_float2(0.f, 0.f);
+          if (lx >= 0 && lx < M && ly >= 0 && ly < M)
+            c0[j] = c_negif(c_mulc(__ldg(Ep + ly * M + lx), __ldg(P + ly * M + lx)), (lx + ly) & 1);
+        }
+      }
+      const bool two = i + 1 < n;
+      if (two) {
+        const int bb = list[i + 1];
+        const int2 c = __ldg(tlb + bb);
+        const int lx = X - c.y;
+        const float2* Ep = Eb + size_t(bb) * M * M;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int ly = Y0 + 8 * j - c.x;
+          c1[j] = make_float2(0.f, 0.f);
+          if (lx >= 0 && lx < M && ly >= 0 && ly < M)
+            c1[j] = c_negif(c_mulc(__ldg(Ep + ly * M + lx), __ldg(P + ly * M + lx)), (lx + ly) & 1);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        acc[j] = c_add(acc[j], c0[j]);
+        if (two) acc[j] = c_add(acc[j], c1[j]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const int Y = Y0 + 8 * j;
+    if (Y < H && X < W) {
+      float2* o = dO + size_t(Y) * W + X;
+      *o = accumulate ? c_add(*o, acc[j]) : acc[j];
+    }
+  }
+}
+
+PTY_DEVI void loss_sum_block(const double* __restrict__ loss_pat, int B, double* loss_total) {
+  __shared__ double red[8];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < B; b += 256) s += loss_pat[b];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < 8; ++i) t += red[i];
+    loss_total[0] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_loss_total(const double* __restrict__ loss_pat, int B,
+                                                    double* __restrict__ loss_total) {
+  loss_sum_block(loss_pat, B, loss_total);
+}
+
+// dP: block (p, g) sums patterns [g*kGroup, (g+1)*kGroup) for kPixBlock probe
+// pixels; the last of the G blocks of pixel block p sums the partials in order.
+__global__ void __launch_bounds__(kPixBlock) k_dP(const float2* __restrict__ Eb, const float2* __restrict__ O,
+                                                  const int2* __restrict__ tlb, int B, int W, int M,
+                                                  float2* __restrict__ part, unsigned* __restrict__ done,
+                                                  float2* __restrict__ dP, int accumulate,
+                                                  const double* __restrict__ loss_pat,
+                                                  double* __restrict__ loss_total) {
+  __shared__ int last;
+  const int p = blockIdx.x, g = blockIdx.y, G = gridDim.y;
+  const int idx = p * kPixBlock + threadIdx.x;
+  const bool in = idx < M * M;
+  const int y = idx / M, x = idx - (idx / M) * M;
+  if (in) {
+    float2 acc = make_float2(0.f, 0.f);
+    const int b1 = min(B, (g + 1) * kGroup);
+    int b = g * kGroup;
+    for (; b + 1 < b1; b += 2) {  // two loads in flight, adds in order
+      const int2 c0 = __ldg(tlb + b), c1 = __ldg(tlb + b + 1);
+      float2 t0 = make_float2(0.f, 0.f), t1 = make_float2(0.f, 0.f);
+      if (c0.x >= 0) t0 = c_mulc(__ldg(Eb + size_t(b) * M * M + idx), __ldg(O + size_t(c0.x + y) * W + c0.y + x));
+      if (c1.x >= 0)
+        t1 = c_mulc(__ldg(Eb + size_t(b + 1) * M * M + idx), __ldg(O + size_t(c1.x + y) * W + c1.y + x));
+      acc = c_add(c_add(acc, t0), t1);
+    }
+    if (b < b1) {
+      const int2 c0 = __ldg(tlb + b);
+      if (c0.x >= 0)
+        acc = c_add(acc, c_mulc(__ldg(Eb + size_t(b) * M * M + idx), __ldg(O + size_t(c0.x + y) * W + c0.y + x)));
+    }
+    __stcg(reinterpret_cast<float2*>(part + size_t(g) * M * M + idx), c_negif(acc, (x + y) & 1));
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(done + p, 1u) == unsigned(G - 1));
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    if (in) {
+      float2 acc = make_float2(0.f, 0.f);
+      for (int gg = 0; gg < G; ++gg) acc = c_add(acc, __ldcg(part + size_t(gg) * M * M + idx));
+      dP[idx] = accumulate ? c_add(dP[idx], acc) : acc;
+    }
+    if (threadIdx.x == 0) done[p] = 0u;  // ready for the next call
+  }
+  if (p == 0 && g == 0 && loss_total) loss_sum_block(loss_pat, B, loss_total);
+}
+
+int launch_assemble(const float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H,
+                    int W, int M, float2* dO, float2* dP, float2* part, unsigned* done,
+                    const double* loss_pat, double* loss_total, bool accumulate, cudaStream_t s) {
+  if (dO) {
+    const int ntx = (W + kTile - 1) / kTile, nty = (H + kTile - 1) / kTile;
+    k_dO<<<ntx * nty, 256, 0, s>>>(Eb, P, tlb, B, H, W, M, ntx, dO, accumulate ? 1 : 0);
+  }
+  if (dP) {
+    const int G = (B + kGroup - 1) / kGroup;
+    dim3 grid(dp_counters(M), G);
+    k_dP<<<grid, kPixBlock, 0, s>>>(Eb, O, tlb, B, W, M, part, done, dP, accumulate ? 1 : 0, loss_pat,
+                                    loss_total);
+  } else if (loss_total) {
+    k_loss_total<<<1, 256, 0, s>>>(loss_pat, B, loss_total);
+  }
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+}  // namespace pty

@@ -28,3 +28,4 @@ static inline bool pty_aligned(const void* p, size_t a) {
   return (reinterpret_cast<uintptr_t>(p) % a) == 0;
 }
 static inline size_t pty_align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+__host__ __device__ constexpr size_t pty_align_up_c(size_t x, size_t a) { return (x + a - 1) / a * a; }

@@ -104,6 +104,8 @@ _status_cache: dict = {}
 def device_status(device) -> torch.Tensor:
     """The per-device int32 status word the kernels raise errors into."""
     device = torch.device(device)
+    if device.index is None:
+        device = torch.device(device.type, torch.cuda.current_device())
     st = _status_cache.get(device)
     if st is None:
         st = torch.zeros(1, dtype=torch.int32, device=device)
@@ -118,6 +120,22 @@ def read_status(device, reset: bool = True) -> int:
     if reset:
         st.zero_()
     return v
+
+
+class FwdAdjWorkspace:
+    """Reusable device scratch for ``ptycho_fwd_adj`` (grows on demand)."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, nbytes: int, device) -> torch.Tensor:
+        nbytes = max(int(nbytes), 256)
+        if self.buf is None or self.buf.numel() < nbytes or self.buf.device != torch.device(device):
+            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        return self.buf
+
+
+_default_ws: dict = {}
 
 
 def _batch_arg(batch, dev):
@@ -146,22 +164,6 @@ def forward_intensity(O: torch.Tensor, P: torch.Tensor, tl: torch.Tensor, batch=
         bt.data_ptr() if bt is not None else None, B, out.data_ptr(), st.data_ptr(),
         _stream_handle(O.device)), "ptycho_forward_intensity")
     return out
-
-
-class FwdAdjWorkspace:
-    """Reusable device scratch for ``ptycho_fwd_adj`` (grows on demand)."""
-
-    def __init__(self):
-        self.buf = None
-
-    def get(self, nbytes: int, device) -> torch.Tensor:
-        nbytes = max(int(nbytes), 256)
-        if self.buf is None or self.buf.numel() < nbytes or self.buf.device != torch.device(device):
-            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
-        return self.buf
-
-
-_default_ws: dict = {}
 
 
 def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = True,
@@ -208,6 +210,68 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
         1 if accumulate else 0, ws.data_ptr(), ws.numel(), st.data_ptr(),
         _stream_handle(dev)), "ptycho_fwd_adj")
     return loss_total, lp, dO, dP
+
+
+class FwdAdjPlan:
+    """Preallocated ``ptycho_fwd_adj`` call for a fixed problem (the training step).
+
+    Holds the object/probe/windows/measurement tensors by reference (update
+    them in place between steps), a static device buffer of ``batch_size``
+    frame ids, the gradient outputs and the workspace.  ``run()`` enqueues one
+    call with no host-side allocation; ``capture()`` records it into a CUDA
+    graph so each step is a single graph launch (``replay()``)."""
+
+    def __init__(self, O, P, tl, Imeas, loss_type: str, batch_size: int, want_dO: bool = True,
+                 want_dP: bool = True, per_pattern: bool = False):
+        if loss_type not in LOSS_CODES:
+            raise ValueError(f"loss_type must be one of {tuple(LOSS_CODES)}")
+        for name, x, dt in (("object", O, torch.complex64), ("probe", P, torch.complex64),
+                            ("windows", tl, torch.int32), ("measurements", Imeas, torch.float32)):
+            if not x.is_cuda or x.dtype != dt or not x.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous CUDA {dt} tensor")
+        self.M = _check_probe(P)
+        self.O, self.P, self.tl, self.Imeas = O, P, tl, Imeas
+        self.dev = O.device
+        H, W = O.shape
+        F = int(tl.shape[0])
+        if Imeas.shape != (F, self.M, self.M):
+            raise ValueError("measurements must be [F, M, M]")
+        self.B = int(batch_size)
+        self.batch = torch.zeros(self.B, dtype=torch.int32, device=self.dev)
+        self.loss_total = torch.zeros((), dtype=torch.float64, device=self.dev)
+        self.loss_per_pattern = (torch.zeros(self.B, dtype=torch.float64, device=self.dev)
+                                 if per_pattern else None)
+        self.dO = torch.zeros((H, W), dtype=torch.complex64, device=self.dev) if want_dO else None
+        self.dP = torch.zeros((self.M, self.M), dtype=torch.complex64, device=self.dev) if want_dP else None
+        nbytes = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, self.M, self.M, self.B))
+        self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.dev)
+        self.status = device_status(self.dev)
+        ptr = lambda x: x.data_ptr() if x is not None else None  # noqa: E731
+        self._args = (O.data_ptr(), H, W, P.data_ptr(), self.M, self.M, tl.data_ptr(), Imeas.data_ptr(), F,
+                      self.batch.data_ptr(), self.B, LOSS_CODES[loss_type], ptr(self.loss_per_pattern),
+                      self.loss_total.data_ptr(), ptr(self.dO), ptr(self.dP), 0, self.ws.data_ptr(),
+                      self.ws.numel(), self.status.data_ptr())
+        self.graph = None
+
+    def set_batch(self, frame_ids) -> None:
+        """Copy the next minibatch's frame ids into the static buffer (stream-ordered)."""
+        self.batch.copy_(torch.as_tensor(frame_ids).to(self.dev, torch.int32), non_blocking=True)
+
+    def run(self) -> None:
+        _lib.check(_lib.lib().ptycho_fwd_adj(*self._args, _stream_handle(self.dev)), "ptycho_fwd_adj")
+
+    def capture(self) -> None:
+        self.run()  # warm: sets kernel attributes outside capture
+        torch.cuda.synchronize(self.dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run()
+        self.graph = g
+
+    def replay(self) -> None:
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
 
 
 # --------------------------------------------------------------------------

@@ -80,7 +80,7 @@ int ptycho_version(void);
  * batched: for b < B, with f = batch[b],
  *   I_out[b] = | fftshift( fft2( P * O[tlY_f : tlY_f+M, tlX_f : tlX_f+N] ) ) |^2
  * O [H][W] complex64, P [M][N] complex64, I_out [B][M][N] float32.
- * Supported: M == N in {64, 128}.
+ * Supported: M == N in {64, 128}.  Needs no scratch memory.
  * ---------------------------------------------------------------------- */
 int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M, int N,
                              const int32_t* tl, int F, const int32_t* batch, int B,
@@ -99,7 +99,8 @@ int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M
  * dP [M][N] may each be NULL to skip that output; when dO and dP are both
  * NULL the adjoint is not computed.  With PTYCHO_FLAG_ACCUMULATE dO/dP are
  * added to instead of overwritten.  workspace: device scratch of at least
- * ptycho_fwd_adj_workspace_size() bytes, 256-byte aligned.
+ * ptycho_fwd_adj_workspace_size() bytes, 256-byte aligned.  Imeas must be
+ * 16-byte aligned (each pattern's measurement is fetched by a bulk copy).
  * ---------------------------------------------------------------------- */
 size_t ptycho_fwd_adj_workspace_size(int H, int W, int M, int N, int B);
 
