@@ -25,6 +25,8 @@ SIGNATURES = {
     "ptycho_fwd_adj_workspace_size": (_c_size, [_c_int, _c_int, _c_int, _c_int, _c_int]),
     "ptycho_fwd_adj": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _c_int,
                                 _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _c_size, _vp, _vp]),
+    "ptycho_fwd_adj_noalloc": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp,
+                                        _c_int, _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _vp]),
 }
 
 _lock = threading.Lock()

@@ -110,6 +110,25 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N,
                    float* dP, unsigned flags, void* workspace, size_t workspace_bytes,
                    int32_t* status_out, ptycho_stream_t stream);
 
+/* ---------------------------------------------------------------------- *
+ * ptycho_fwd_adj without a workspace, for callers that cannot allocate
+ * device memory (an FFI host with no CUDA allocator of its own, a step that
+ * must not trigger an allocation's device synchronisation).  No counterpart
+ * in the reference.  Same arguments and results as ptycho_fwd_adj minus the
+ * workspace: the scratch is a 48 MiB static device array inside this
+ * library, held by every GPU that loads it until the process exits.  A call
+ * needing more than 48 MiB of scratch (ptycho_fwd_adj_workspace_size) returns
+ * PTYCHO_ERR_WORKSPACE without touching the device (M = 128 fits up to about
+ * 360 patterns per call).  The first call on a device looks up the array's
+ * address; make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race, so order them on one stream.
+ * ---------------------------------------------------------------------- */
+int ptycho_fwd_adj_noalloc(const float* O, int H, int W, const float* P, int M, int N,
+                           const int32_t* tl, const float* Imeas, int F, const int32_t* batch,
+                           int B, int loss_type, double* loss_per_pattern, double* loss_total,
+                           float* dO, float* dP, unsigned flags, int32_t* status_out,
+                           ptycho_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
