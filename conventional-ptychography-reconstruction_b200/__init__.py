@@ -6,11 +6,15 @@ The directory name is not a Python identifier; import it with
 ``importlib.import_module("conventional-ptychography-reconstruction_b200")``.
 """
 from . import _lib, optics, synth
+from . import adam, cmlp, complex_inr, hashgrid
+from .adam import FusedAdam
+from .complex_inr import ComplexINRModel2D
+from .hashgrid import Encoding
 from .optics import (LOSS_CODES, forward_imaging_model, forward_intensity, forward_intensity_batched,
                      fused_loss, fwd_adj_raw, make_windows, check_windows, read_status,
                      scan_positions_to_pixels)
 
-__all__ = ["LOSS_CODES", "forward_imaging_model", "forward_intensity", "forward_intensity_batched",
+__all__ = ["FusedAdam", "ComplexINRModel2D", "Encoding", "LOSS_CODES", "forward_imaging_model", "forward_intensity", "forward_intensity_batched",
            "fused_loss", "fwd_adj_raw", "make_windows", "check_windows", "read_status",
            "scan_positions_to_pixels", "lib"]
 

@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(_HERE, "libptycho_b200.so")
 
 _c_int, _c_size, _vp = ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p
 _c_uint, _c_float, _c_double = ctypes.c_uint, ctypes.c_float, ctypes.c_double
+_c_ll = ctypes.c_longlong
+_pp = ctypes.POINTER(ctypes.c_void_p)
 
 # name -> (restype, argtypes); every entry is declared in include/ptycho_b200.h
 SIGNATURES = {
@@ -25,6 +27,20 @@ SIGNATURES = {
     "ptycho_fwd_adj_workspace_size": (_c_size, [_c_int, _c_int, _c_int, _c_int, _c_int]),
     "ptycho_fwd_adj": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _c_int,
                                 _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _c_size, _vp, _vp]),
+    "ptycho_hashgrid_entries": (_c_int, [_c_int, _c_int, _c_int, _c_float]),
+    "ptycho_hashgrid_forward": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
+    "ptycho_hashgrid_contrib": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp, _vp]),
+    "ptycho_hashgrid_segments": (_c_int, [_vp, _c_ll, _c_int, _vp, _vp]),
+    "ptycho_hashgrid_backward": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp,
+                                          _c_int, _vp]),
+    "ptycho_cmlp_packed_bytes": (_c_size, []),
+    "ptycho_cmlp_grad_floats": (_c_int, []),
+    "ptycho_cmlp_pack": (_c_int, [_vp] * 12 + [_vp]),
+    "ptycho_cmlp_forward": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp]),
+    "ptycho_cmlp_backward_workspace_size": (_c_size, [_c_int]),
+    "ptycho_cmlp_backward": (_c_int, [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _c_size, _vp, _vp]),
+    "ptycho_adam_step": (_c_int, [_pp, _pp, _pp, _pp, ctypes.POINTER(_c_ll), _c_int, _c_int, _c_float, _c_float,
+                                  _c_float, _c_float, _vp]),
     "ptycho_fwd_adj_noalloc": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp,
                                         _c_int, _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _vp]),
 }

@@ -1,0 +1,128 @@
+"""ComplexINRModel2D on the B200 kernels -- mirrors models/complex_inr.py:85-334.
+
+Same constructor, attributes (``xy_coords``, ``probe_coords``,
+``k_object``, ``k_probe``, ``has_*_residual``, ``downsampled_*``) and
+``forward() -> (object_complex [W, H], probe_complex [Wp, Hp] or None)``.
+The hash encoders are :class:`hashgrid.Encoding` (tiny-cuda-nn's interface)
+and the MLPs :class:`cmlp.ComplexMLP` (fused tensor-core kernels).  The
+Fourier upsampling of the object (models/complex_inr.py:252-271) uses the
+same torch.fft formula as the reference.
+"""
+from __future__ import annotations
+
+import torch
+import torch.nn as nn
+import torch.nn.functional as F
+
+from .cmlp import ComplexMLP
+from .hashgrid import Encoding
+
+
+class ComplexINRModel2D(nn.Module):
+    def __init__(self, output_width, output_height, downsample_factor, update_probe=True, probe_width=None,
+                 probe_height=None, n_levels=16, n_features_per_level=2, log2_hashmap_size=19,
+                 base_resolution=16, per_level_scale=1.5, first_omega_0=10.0, hidden_omega_0=10.0,
+                 hidden_features=64, hidden_layers=2, trainable_omega0=False, use_residual=False,
+                 object_initial=None, probe_initial=None):
+        super().__init__()
+        self.update_probe = update_probe
+        self.use_residual = use_residual
+        self.output_width = output_width
+        self.output_height = output_height
+        self.probe_width = probe_width if probe_width is not None else output_width
+        self.probe_height = probe_height if probe_height is not None else output_height
+        self.num_features = n_levels * n_features_per_level
+        encoding_config = {"otype": "HashGrid", "n_levels": n_levels, "n_features_per_level": n_features_per_level,
+                           "log2_hashmap_size": log2_hashmap_size, "base_resolution": base_resolution,
+                           "per_level_scale": per_level_scale}
+        self.xy_hash_encoder = Encoding(n_input_dims=2, encoding_config=encoding_config)
+        self.probe_hash_encoder = (Encoding(n_input_dims=2, encoding_config=encoding_config.copy(), seed=7331)
+                                   if update_probe else None)
+        self.object_complex_mlp = ComplexMLP(self.num_features, hidden_features, hidden_layers, 1,
+                                             first_omega_0=first_omega_0, hidden_omega_0=hidden_omega_0,
+                                             trainable_omega0=trainable_omega0)
+        self.probe_complex_mlp = (ComplexMLP(self.num_features, hidden_features, hidden_layers, 1,
+                                             first_omega_0=first_omega_0, hidden_omega_0=hidden_omega_0,
+                                             trainable_omega0=trainable_omega0) if update_probe else None)
+        self.init_scale_grids(downsample_factor)
+        if self.use_residual:
+            self.init_residual_params(object_initial, probe_initial)
+
+    def init_scale_grids(self, downsample_factor):
+        """Pixel-centre coordinates; element [i, j] of the reshaped output gets
+        encoder input (dim0 = (j + 0.5) / H, dim1 = (i + 0.5) / W)."""
+        dw = self.output_width // downsample_factor
+        dh = self.output_height // downsample_factor
+        xs = torch.linspace(0.5 / dw, 1 - 0.5 / dw, dw)
+        ys = torch.linspace(0.5 / dh, 1 - 0.5 / dh, dh)
+        xv, yv = torch.meshgrid([xs, ys], indexing="ij")
+        self.downsampled_width = dw
+        self.downsampled_height = dh
+        self.xy_coords = nn.Parameter(torch.stack((yv.flatten(), xv.flatten())).t().contiguous(),
+                                      requires_grad=False)
+        if self.update_probe:
+            xs = torch.linspace(0.5 / self.probe_width, 1 - 0.5 / self.probe_width, self.probe_width)
+            ys = torch.linspace(0.5 / self.probe_height, 1 - 0.5 / self.probe_height, self.probe_height)
+            xv, yv = torch.meshgrid([xs, ys], indexing="ij")
+            self.probe_coords = nn.Parameter(torch.stack((yv.flatten(), xv.flatten())).t().contiguous(),
+                                             requires_grad=False)
+        else:
+            self.probe_coords = None
+        self.downsample_factor = downsample_factor
+
+    def init_residual_params(self, object_initial, probe_initial):
+        """output = k * network + initial, k a real parameter initialised to 1e-8
+        (models/complex_inr.py:209-250)."""
+        if object_initial is not None:
+            if not torch.is_complex(object_initial):
+                raise ValueError("object_initial must be a complex tensor")
+            self.register_buffer("object_initial", object_initial.clone())
+            self.k_object = nn.Parameter(torch.tensor(1e-8, dtype=torch.float32))
+            self.has_object_residual = True
+        else:
+            self.has_object_residual = False
+        if self.update_probe and probe_initial is not None:
+            if not torch.is_complex(probe_initial):
+                raise ValueError("probe_initial must be a complex tensor")
+            self.register_buffer("probe_initial", probe_initial.clone())
+            self.k_probe = nn.Parameter(torch.tensor(1e-8, dtype=torch.float32))
+            self.has_probe_residual = True
+        else:
+            self.has_probe_residual = False
+
+    def fourier_upsample(self, x, scale_factor):
+        """fftshift(fft2) -> zero-pad -> ifftshift -> ifft2, times scale^2 (:252-271)."""
+        B, C, H, W = x.shape
+        x_fft = torch.fft.fftshift(torch.fft.fft2(x, dim=(-2, -1)), dim=(-2, -1))
+        nH, nW = int(H * scale_factor), int(W * scale_factor)
+        ph, pw = (nH - H) // 2, (nW - W) // 2
+        x_fft = F.pad(x_fft, (pw, nW - W - pw, ph, nH - H - ph), mode="constant", value=0)
+        x_up = torch.fft.ifft2(torch.fft.ifftshift(x_fft, dim=(-2, -1)), dim=(-2, -1))
+        return x_up * (scale_factor ** 2)
+
+    def forward(self):
+        xy = self.xy_coords if self.xy_coords.is_cuda else self.xy_coords.cuda()
+        feats = self.xy_hash_encoder(xy).float()
+        obj = self._get_complex_output(self.object_complex_mlp, feats)
+        obj = obj.reshape(self.downsampled_width, self.downsampled_height)
+        obj = self.fourier_upsample(obj.unsqueeze(0).unsqueeze(0), self.downsample_factor).squeeze(0).squeeze(0)
+        if self.update_probe:
+            pc = self.probe_coords if self.probe_coords.is_cuda else self.probe_coords.cuda()
+            pf = self.probe_hash_encoder(pc).float()
+            probe = self._get_complex_output(self.probe_complex_mlp, pf).reshape(self.probe_width,
+                                                                                 self.probe_height)
+        else:
+            probe = None
+        if self.use_residual:
+            obj = self.apply_residual(obj, is_object=True)
+            if self.update_probe and probe is not None:
+                probe = self.apply_residual(probe, is_object=False)
+        return obj, probe
+
+    def _get_complex_output(self, model, coords):
+        return model.net(coords)
+
+    def apply_residual(self, complex_tensor, is_object=True):
+        if is_object:
+            return self.k_object * complex_tensor + self.object_initial if self.has_object_residual else complex_tensor
+        return self.k_probe * complex_tensor + self.probe_initial if self.has_probe_residual else complex_tensor

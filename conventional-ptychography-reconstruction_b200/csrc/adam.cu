@@ -1,0 +1,76 @@
+// adam.cu -- fused multi-tensor Adam step (torch.optim.Adam semantics).
+//
+// Replaces optimizer.step() of Recovery.py:321 (Adam built at :238-241) for
+// float32 parameter tensors; complex parameters are passed as their real
+// view, so real and imaginary parts get independent moments exactly as
+// torch.optim.Adam treats complex tensors.  Per element, with t = step:
+//   m = m + (1 - b1) (g - m);  v = b2 v + (1 - b2) g^2
+//   p = p - (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps)
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace pty {
+
+constexpr int kAdamMaxTensors = 48;
+
+struct AdamList {
+  float* p[kAdamMaxTensors];
+  const float* g[kAdamMaxTensors];
+  float* m[kAdamMaxTensors];
+  float* v[kAdamMaxTensors];
+  long long end[kAdamMaxTensors];  // cumulative element counts
+  int n;
+};
+
+__global__ void __launch_bounds__(256) k_adam(const AdamList L, long long total, float lr_bc1, float b1, float b2,
+                                              float inv_sqrt_bc2, float eps) {
+  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < total; i += (long long)gridDim.x * 256) {
+    int k = 0;
+    while (L.end[k] <= i) ++k;
+    const long long j = i - (k ? L.end[k - 1] : 0);
+    const float g = L.g[k][j];
+    float m = L.m[k][j], v = L.v[k][j];
+    m = fmaf(1.0f - b1, g - m, m);
+    v = fmaf(1.0f - b2, g * g, b2 * v);
+    const float denom = sqrtf(v) * inv_sqrt_bc2 + eps;
+    L.p[k][j] -= lr_bc1 * (m / denom);
+    L.m[k][j] = m;
+    L.v[k][j] = v;
+  }
+}
+
+}  // namespace pty
+
+using namespace pty;
+
+extern "C" int ptycho_adam_step(float* const* params, const float* const* grads, float* const* exp_avg,
+                                float* const* exp_avg_sq, const long long* numels, int n_tensors, int step,
+                                float lr, float beta1, float beta2, float eps, ptycho_stream_t stream) {
+  if (n_tensors < 0 || n_tensors > kAdamMaxTensors || step < 1 || !(lr >= 0.f)) return PTYCHO_ERR_INVALID_ARG;
+  if (n_tensors == 0) return PTYCHO_OK;
+  if (!params || !grads || !exp_avg || !exp_avg_sq || !numels) return PTYCHO_ERR_INVALID_ARG;
+  AdamList L{};
+  long long total = 0;
+  for (int k = 0; k < n_tensors; ++k) {
+    if (numels[k] < 0 || (numels[k] > 0 && (!params[k] || !grads[k] || !exp_avg[k] || !exp_avg_sq[k])))
+      return PTYCHO_ERR_INVALID_ARG;
+    L.p[k] = params[k];
+    L.g[k] = grads[k];
+    L.m[k] = exp_avg[k];
+    L.v[k] = exp_avg_sq[k];
+    total += numels[k];
+    L.end[k] = total;
+  }
+  L.n = n_tensors;
+  if (total == 0) return PTYCHO_OK;
+  const double bc1 = 1.0 - pow((double)beta1, (double)step);
+  const double bc2 = 1.0 - pow((double)beta2, (double)step);
+  const long long blocks = (total + 255) / 256;
+  const int grid = (int)(blocks < 148 * 16 ? blocks : 148 * 16);
+  k_adam<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(L, total, (float)(lr / bc1), beta1, beta2,
+                                                                   (float)(1.0 / sqrt(bc2)), eps);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}

@@ -1,0 +1,265 @@
+// hashgrid.cu -- multi-resolution hash encoding (forward, deterministic backward).
+//
+// Replaces the tiny-cuda-nn HashGrid encoding the reference consumes at
+// models/complex_inr.py:130-145 (called at :279 and :294): 2-D coordinates
+// in [0,1] -> n_levels x F features.  Level l has scale
+// s_l = base * per_level_scale^l - 1 and r_l = ceil(s_l) + 1 vertices per
+// axis; a coordinate maps to x * s_l + 0.5, whose floor is the cell corner and
+// whose fraction gives the bilinear weights.  A level whose r_l^2 (rounded up
+// to a multiple of 8) fits in T = 2^log2_hashmap_size entries is indexed
+// densely (ix + iy * r_l), otherwise by (ix * 1) ^ (iy * 2654435761) mod T.
+// Level l's entries start at the sum of the previous levels' entry counts;
+// each entry holds F = 2 floats (the table is [entries][2] float32).
+//
+// Backward: the coordinates of an INR are fixed, so the (entry, coordinate,
+// weight) contributions are static.  ptycho_hashgrid_contrib emits them; the
+// caller sorts them by entry once (stable) and passes the CSR to
+// ptycho_hashgrid_backward, which gathers each entry's contributions in that
+// fixed order -- a deterministic table-gradient "scatter" without atomics.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace pty {
+
+constexpr int kMaxLevels = 32;
+constexpr uint32_t kPrimeY = 2654435761u;
+
+struct LevelTable {
+  float scale[kMaxLevels];
+  int res[kMaxLevels];
+  int n[kMaxLevels];       // entries in the level
+  int offset[kMaxLevels];  // first entry of the level
+  int dense[kMaxLevels];
+  int levels;
+  int total;  // total entries
+};
+
+static int make_levels(int n_levels, int log2_T, int base_res, float per_level_scale, LevelTable* L) {
+  if (n_levels < 1 || n_levels > kMaxLevels || log2_T < 4 || log2_T > 26 || base_res < 1 ||
+      !(per_level_scale >= 1.0f))
+    return PTYCHO_ERR_INVALID_ARG;
+  const long long T = 1ll << log2_T;
+  long long off = 0;
+  for (int l = 0; l < n_levels; ++l) {
+    const double scale = double(base_res) * pow(double(per_level_scale), double(l)) - 1.0;
+    const long long res = (long long)ceil(scale) + 1;
+    long long dn = res * res;
+    dn = (dn + 7) / 8 * 8;
+    const long long n = dn < T ? dn : T;
+    L->scale[l] = (float)scale;
+    L->res[l] = (int)res;
+    L->n[l] = (int)n;
+    L->offset[l] = (int)off;
+    L->dense[l] = dn <= T;
+    off += n;
+  }
+  L->levels = n_levels;
+  L->total = (int)off;
+  return off < (1ll << 31) ? PTYCHO_OK : PTYCHO_ERR_INVALID_ARG;
+}
+
+PTY_DEVI int corner_entry(const LevelTable& L, int l, int cx, int cy) {
+  uint32_t e;
+  if (L.dense[l]) e = uint32_t(cx) + uint32_t(cy) * uint32_t(L.res[l]);
+  else e = uint32_t(cx) ^ (uint32_t(cy) * kPrimeY);
+  return L.offset[l] + int(e % uint32_t(L.n[l]));
+}
+
+// one thread per (coordinate, level): 4 corner gathers of float2, bilinear blend
+__global__ void __launch_bounds__(256) k_hash_fwd(const float2* __restrict__ coords, int N,
+                                                  const float2* __restrict__ table, const LevelTable L,
+                                                  float2* __restrict__ feat) {
+  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (i >= (long long)N * L.levels) return;
+  const int n = int(i / L.levels), l = int(i - (long long)n * L.levels);
+  const float2 x = __ldg(coords + n);
+  const float s = L.scale[l];
+  const float px = fmaf(x.x, s, 0.5f), py = fmaf(x.y, s, 0.5f);
+  const float gx = floorf(px), gy = floorf(py);
+  const float fx = px - gx, fy = py - gy;
+  const int ix = int(gx), iy = int(gy);
+  const float2 t00 = __ldg(table + corner_entry(L, l, ix, iy));
+  const float2 t10 = __ldg(table + corner_entry(L, l, ix + 1, iy));
+  const float2 t01 = __ldg(table + corner_entry(L, l, ix, iy + 1));
+  const float2 t11 = __ldg(table + corner_entry(L, l, ix + 1, iy + 1));
+  const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
+  float2 o;
+  o.x = fmaf(w11, t11.x, fmaf(w01, t01.x, fmaf(w10, t10.x, w00 * t00.x)));
+  o.y = fmaf(w11, t11.y, fmaf(w01, t01.y, fmaf(w10, t10.y, w00 * t00.y)));
+  feat[(long long)n * L.levels + l] = o;
+}
+
+// contributions: for coordinate n, level l, corner k -> key = entry,
+// item = n * levels + l (feature pair index), weight
+__global__ void __launch_bounds__(256) k_hash_contrib(const float2* __restrict__ coords, int N, const LevelTable L,
+                                                      int* __restrict__ key, int* __restrict__ item,
+                                                      float* __restrict__ weight) {
+  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (i >= (long long)N * L.levels) return;
+  const int n = int(i / L.levels), l = int(i - (long long)n * L.levels);
+  const float2 x = __ldg(coords + n);
+  const float s = L.scale[l];
+  const float px = fmaf(x.x, s, 0.5f), py = fmaf(x.y, s, 0.5f);
+  const float gx = floorf(px), gy = floorf(py);
+  const float fx = px - gx, fy = py - gy;
+  const int ix = int(gx), iy = int(gy);
+  const long long base = i * 4;
+  const int it = n * L.levels + l;
+  key[base + 0] = corner_entry(L, l, ix, iy);
+  key[base + 1] = corner_entry(L, l, ix + 1, iy);
+  key[base + 2] = corner_entry(L, l, ix, iy + 1);
+  key[base + 3] = corner_entry(L, l, ix + 1, iy + 1);
+  weight[base + 0] = (1.f - fx) * (1.f - fy);
+  weight[base + 1] = fx * (1.f - fy);
+  weight[base + 2] = (1.f - fx) * fy;
+  weight[base + 3] = fx * fy;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) item[base + k] = it;
+}
+
+// segment starts from sorted keys: start[e] = first position with key >= e
+__global__ void __launch_bounds__(256) k_seg_starts(const int* __restrict__ skey, long long K, int E,
+                                                    int* __restrict__ start) {
+  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (i > K) return;
+  const int prev = i == 0 ? -1 : skey[i - 1];
+  const int cur = i == K ? E : skey[i];
+  for (int e = prev + 1; e <= cur; ++e) start[e] = int(i);
+}
+
+// long segments (coarse levels): one warp per entry, lanes stride the segment
+// in order, fixed xor tree
+__global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ start, const int* __restrict__ item,
+                                                       const float* __restrict__ weight,
+                                                       const float2* __restrict__ dfeat, int E,
+                                                       float2* __restrict__ dtable, int accumulate) {
+  const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (e >= E) return;
+  const int s0 = start[e], s1 = start[e + 1];
+  float ax = 0.f, ay = 0.f;
+  for (int j = s0 + lane; j < s1; j += 32) {
+    const float w = __ldg(weight + j);
+    const float2 g = __ldg(dfeat + __ldg(item + j));
+    ax = fmaf(w, g.x, ax);
+    ay = fmaf(w, g.y, ay);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+  }
+  if (lane == 0) {
+    float2 r = make_float2(ax, ay);
+    if (accumulate) {
+      const float2 old = dtable[e];
+      r = make_float2(old.x + r.x, old.y + r.y);
+    }
+    dtable[e] = r;
+  }
+}
+
+// short segments (fine levels): one thread per entry, sequential in order
+__global__ void __launch_bounds__(256) k_hash_bwd_thread(const int* __restrict__ start, const int* __restrict__ item,
+                                                         const float* __restrict__ weight,
+                                                         const float2* __restrict__ dfeat, int e0, int E,
+                                                         float2* __restrict__ dtable, int accumulate) {
+  const int e = e0 + blockIdx.x * 256 + threadIdx.x;
+  if (e >= E) return;
+  const int s0 = start[e], s1 = start[e + 1];
+  float ax = 0.f, ay = 0.f;
+  for (int j = s0; j < s1; ++j) {
+    const float w = __ldg(weight + j);
+    const float2 g = __ldg(dfeat + __ldg(item + j));
+    ax = fmaf(w, g.x, ax);
+    ay = fmaf(w, g.y, ay);
+  }
+  float2 r = make_float2(ax, ay);
+  if (accumulate) {
+    const float2 old = dtable[e];
+    r = make_float2(old.x + r.x, old.y + r.y);
+  }
+  dtable[e] = r;
+}
+
+}  // namespace pty
+
+using namespace pty;
+
+extern "C" {
+
+int ptycho_hashgrid_entries(int n_levels, int log2_hashmap_size, int base_resolution, float per_level_scale) {
+  LevelTable L;
+  if (make_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scale, &L)) return -1;
+  return L.total;
+}
+
+int ptycho_hashgrid_forward(const float* coords, int N, const float* table, int n_levels,
+                            int log2_hashmap_size, int base_resolution, float per_level_scale,
+                            float* features, ptycho_stream_t stream) {
+  LevelTable L;
+  int st = make_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scale, &L);
+  if (st) return st;
+  if (N < 0 || (N > 0 && (!coords || !table || !features))) return PTYCHO_ERR_INVALID_ARG;
+  if (!pty_aligned(coords, 8) || !pty_aligned(table, 8) || !pty_aligned(features, 8))
+    return PTYCHO_ERR_MISALIGNED;
+  if (N == 0) return PTYCHO_OK;
+  const long long work = (long long)N * n_levels;
+  k_hash_fwd<<<(unsigned)((work + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      reinterpret_cast<const float2*>(coords), N, reinterpret_cast<const float2*>(table), L,
+      reinterpret_cast<float2*>(features));
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+int ptycho_hashgrid_contrib(const float* coords, int N, int n_levels, int log2_hashmap_size,
+                            int base_resolution, float per_level_scale, int32_t* key, int32_t* item,
+                            float* weight, ptycho_stream_t stream) {
+  LevelTable L;
+  int st = make_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scale, &L);
+  if (st) return st;
+  if (N < 0 || (N > 0 && (!coords || !key || !item || !weight))) return PTYCHO_ERR_INVALID_ARG;
+  if ((long long)N * n_levels * 4 >= (1ll << 31)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  if (N == 0) return PTYCHO_OK;
+  const long long work = (long long)N * n_levels;
+  k_hash_contrib<<<(unsigned)((work + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      reinterpret_cast<const float2*>(coords), N, L, key, item, weight);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+int ptycho_hashgrid_segments(const int32_t* sorted_key, long long K, int n_entries, int32_t* start,
+                             ptycho_stream_t stream) {
+  if (K < 0 || n_entries < 1 || !start || (K > 0 && !sorted_key)) return PTYCHO_ERR_INVALID_ARG;
+  k_seg_starts<<<(unsigned)((K + 1 + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      sorted_key, K, n_entries, start);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+int ptycho_hashgrid_backward(const int32_t* start, const int32_t* item, const float* weight,
+                             const float* dfeatures, int N, int n_levels, int log2_hashmap_size,
+                             int base_resolution, float per_level_scale, float* dtable, int accumulate,
+                             ptycho_stream_t stream) {
+  LevelTable L;
+  int st = make_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scale, &L);
+  if (st) return st;
+  if (N < 0 || !start || !item || !weight || !dfeatures || !dtable) return PTYCHO_ERR_INVALID_ARG;
+  if (!pty_aligned(dfeatures, 8) || !pty_aligned(dtable, 8)) return PTYCHO_ERR_MISALIGNED;
+  // levels whose average segment is long go to the warp-per-entry kernel
+  int split = 0;
+  for (int l = 0; l < L.levels; ++l)
+    if ((long long)N * 4 >= 16ll * L.n[l]) split = L.offset[l] + L.n[l];
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (split > 0)
+    k_hash_bwd_warp<<<(split + 7) / 8, 256, 0, s>>>(start, item, weight,
+                                                   reinterpret_cast<const float2*>(dfeatures), split,
+                                                   reinterpret_cast<float2*>(dtable), accumulate);
+  if (L.total > split)
+    k_hash_bwd_thread<<<(L.total - split + 255) / 256, 256, 0, s>>>(
+        start, item, weight, reinterpret_cast<const float2*>(dfeatures), split, L.total,
+        reinterpret_cast<float2*>(dtable), accumulate);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+}  // extern "C"

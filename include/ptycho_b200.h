@@ -111,6 +111,84 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N,
                    int32_t* status_out, ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Multi-resolution hash encoding.  Replaces the tiny-cuda-nn
+ * `tcnn.Encoding(n_input_dims=2, {"otype": "HashGrid", ...})` of
+ * models/complex_inr.py:130-145 (called at :279, :294).  coords [N][2]
+ * float32 in [0,1]; table [entries][2] float32 (entries =
+ * ptycho_hashgrid_entries()); features [N][n_levels*2] float32.
+ * Level l: scale s = base*per_level_scale^l - 1, r = ceil(s)+1 vertices per
+ * axis, position x*s + 0.5, bilinear weights; dense index ix + iy*r when
+ * r^2 (rounded up to a multiple of 8) fits in 2^log2_hashmap_size entries,
+ * otherwise (ix ^ iy*2654435761) mod 2^log2_hashmap_size.
+ * ---------------------------------------------------------------------- */
+int ptycho_hashgrid_entries(int n_levels, int log2_hashmap_size, int base_resolution,
+                            float per_level_scale);
+
+int ptycho_hashgrid_forward(const float* coords, int N, const float* table, int n_levels,
+                            int log2_hashmap_size, int base_resolution, float per_level_scale,
+                            float* features, ptycho_stream_t stream);
+
+/* Static contributions of fixed coordinates: for each (coordinate n,
+ * level l, corner k), index i = (n*n_levels + l)*4 + k: key[i] = table entry,
+ * item[i] = n*n_levels + l (feature pair), weight[i] = bilinear weight.
+ * Sort (key, item, weight) by key, stably, once; then pass the segment
+ * starts of ptycho_hashgrid_segments to ptycho_hashgrid_backward. */
+int ptycho_hashgrid_contrib(const float* coords, int N, int n_levels, int log2_hashmap_size,
+                            int base_resolution, float per_level_scale, int32_t* key,
+                            int32_t* item, float* weight, ptycho_stream_t stream);
+
+/* start [n_entries + 1]: start[e] = first sorted position whose key >= e. */
+int ptycho_hashgrid_segments(const int32_t* sorted_key, long long K, int n_entries,
+                             int32_t* start, ptycho_stream_t stream);
+
+/* dtable[e] (+)= sum over e's contributions, in sorted order, of
+ * weight * dfeatures[item]: the table-gradient scatter as a deterministic
+ * gather (no atomics). */
+int ptycho_hashgrid_backward(const int32_t* start, const int32_t* item, const float* weight,
+                             const float* dfeatures, int N, int n_levels, int log2_hashmap_size,
+                             int base_resolution, float per_level_scale, float* dtable,
+                             int accumulate, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
+ * Complex-exponential MLP on the tensor cores (tcgen05, BF16 operands, FP32
+ * accumulation).  Replaces ComplexMLP.net (models/complex_inr.py:6-82,
+ * :308-314) for 32 input features, hidden_features 64, hidden_layers 2.
+ * ptycho_cmlp_pack converts torch-layout parameters (W1 [32][32] f32,
+ * b1 [32] f32, omega1 [1] f32, W2/W3 [32][32] complex64, b2/b3 [32]
+ * complex64, omega2/3 [1] f32, Wo [1][32] complex64, bo [1] complex64)
+ * into an operand blob of ptycho_cmlp_packed_bytes() bytes.
+ * forward: x [N][32] f32 -> y [N] complex64.
+ * backward: recomputes the forward and returns, for upstream gy [N]
+ * complex64, gx [N][32] (may be NULL), y (may be NULL) and the parameter
+ * gradients in `grad` (ptycho_cmlp_grad_floats() floats, torch complex
+ * convention): W1 @0 [32][32], b1 @1024, omega1 @1056, W2 @1058 [32][32]
+ * complex, b2 @3106 complex, omega2 @3170, W3 @3172, b3 @5220, omega3 @5284,
+ * Wo @5286 [32] complex, bo @5350 complex.  Deterministic (per-CTA partial
+ * accumulators summed in a fixed order).
+ * ---------------------------------------------------------------------- */
+size_t ptycho_cmlp_packed_bytes(void);
+int ptycho_cmlp_grad_floats(void);
+int ptycho_cmlp_pack(const float* W1, const float* b1, const float* omega1, const float* W2,
+                     const float* b2, const float* omega2, const float* W3, const float* b3,
+                     const float* omega3, const float* Wo, const float* bo, void* packed,
+                     ptycho_stream_t stream);
+int ptycho_cmlp_forward(const void* packed, const float* x, int N, float* y, int32_t* status_out,
+                        ptycho_stream_t stream);
+size_t ptycho_cmlp_backward_workspace_size(int N);
+int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, int N, float* gx,
+                         float* grad, float* y, void* workspace, size_t workspace_bytes,
+                         int32_t* status_out, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
+ * Fused Adam step over up to 48 float32 tensors (torch.optim.Adam,
+ * Recovery.py:238-241,321; complex parameters as their real view).  The
+ * pointer arrays and numels are host arrays; the tensors are device memory.
+ * ---------------------------------------------------------------------- */
+int ptycho_adam_step(float* const* params, const float* const* grads, float* const* exp_avg,
+                     float* const* exp_avg_sq, const long long* numels, int n_tensors, int step,
+                     float lr, float beta1, float beta2, float eps, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
  * must not trigger an allocation's device synchronisation).  No counterpart

@@ -1,0 +1,188 @@
+"""GPU parity of the INR kernels: HashGrid forward/backward, the tcgen05
+complex MLP forward/backward, fused Adam, and the ComplexINRModel2D mirror.
+
+Tolerances:
+  HashGrid features / table gradient (FP32 vs FP64):            rel-to-max <= 1e-5
+  MLP vs the oracle with the kernel's BF16 operand rounding:      rel-to-max <= 5e-3
+  MLP vs the unrounded FP64 oracle (the reference's arithmetic):  rel-to-max <= 5e-2
+  Adam vs torch.optim.Adam (FP32):                                 rel <= 1e-5
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, load_pkg
+from oracle import inr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    return load_pkg()
+
+
+def rel_max(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+HASH_CFGS = [(8, 12, 4, 1.7), (16, 18, 16, (512 / 16) ** (1 / 15)), (16, 14, 16, 1.5)]
+
+
+@pytest.mark.parametrize("cfg", HASH_CFGS)
+def test_hashgrid_forward_backward(pkg, cfg):
+    L, log2T, base, pls = cfg
+    dev = torch.device("cuda")
+    enc = pkg.Encoding(2, {"otype": "HashGrid", "n_levels": L, "n_features_per_level": 2,
+                           "log2_hashmap_size": log2T, "base_resolution": base, "per_level_scale": pls}).to(dev)
+    with torch.no_grad():
+        enc.params.uniform_(-1, 1)
+    rng = np.random.default_rng(0)
+    n = 48
+    g = (np.arange(n) + 0.5) / n
+    grid = np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+    coords = np.concatenate([rng.random((3000, 2)), grid]).astype(np.float32)
+    ct = torch.from_numpy(coords).to(dev)
+    f = enc(ct)
+    levels = inr.hashgrid_levels(L, log2T, base, pls)
+    assert sum(l[2] for l in levels) == enc.n_entries
+    table = enc.params.detach().cpu().numpy().astype(np.float64)
+    ref = inr.hashgrid_encode(coords.astype(np.float64), table, levels)
+    assert rel_max(f.detach().cpu().numpy(), ref) <= 1e-5
+    gfeat = torch.from_numpy(rng.standard_normal(f.shape).astype(np.float32)).to(dev)
+    f.backward(gfeat)
+    gref = inr.hashgrid_backward(coords.astype(np.float64), gfeat.cpu().numpy(), levels, enc.n_entries)
+    assert rel_max(enc.params.grad.cpu().numpy(), gref) <= 1e-5
+    # deterministic: a second backward gives identical bits
+    g1 = enc.params.grad.clone()
+    enc.params.grad = None
+    enc(ct).backward(gfeat)
+    assert torch.equal(g1, enc.params.grad)
+
+
+def _mlp_from_golden(pkg, k, dev):
+    g = golden("complex_mlp.npz")
+    cfg = g[f"m{k}/cfg"]
+    mlp = pkg.cmlp.ComplexMLP(32, int(cfg[0]), int(cfg[1]), 1, first_omega_0=float(cfg[2]),
+                              hidden_omega_0=float(cfg[3]), trainable_omega0=True).to(dev)
+    with torch.no_grad():
+        for name, p in mlp.named_parameters():
+            src = g[f"m{k}/param/{name}"]
+            p.copy_(torch.from_numpy(src.astype(np.complex64 if p.is_complex() else np.float32)))
+    params = {"W1": g[f"m{k}/param/net.0.linear.weight"], "b1": g[f"m{k}/param/net.0.linear.bias"],
+              "w1": float(g[f"m{k}/param/net.0.omega_0"][0]),
+              "Wh": [g[f"m{k}/param/net.{i}.linear.weight"] for i in (1, 2)],
+              "bh": [g[f"m{k}/param/net.{i}.linear.bias"] for i in (1, 2)],
+              "wh": [float(g[f"m{k}/param/net.{i}.omega_0"][0]) for i in (1, 2)],
+              "Wo": g[f"m{k}/param/net.3.weight"], "bo": g[f"m{k}/param/net.3.bias"]}
+    # the kernel computes on the float32 parameter values
+    f32 = lambda a: np.asarray(a).astype(np.complex64 if np.iscomplexobj(a) else np.float32)  # noqa: E731
+    params = {k2: ([f32(a) for a in v] if isinstance(v, list) else (f32(v) if not isinstance(v, float) else v))
+              for k2, v in params.items()}
+    return mlp, params
+
+
+@pytest.mark.parametrize("N", [50, 1000, 128 * 148 + 37])
+def test_cmlp_forward_backward_against_oracle(pkg, N):
+    dev = torch.device("cuda")
+    mlp, params = _mlp_from_golden(pkg, 0, dev)
+    rng = np.random.default_rng(N)
+    x = (rng.standard_normal((N, 32)) * 0.05 + rng.uniform(-1e-4, 1e-4, (N, 32))).astype(np.float32)
+    xt = torch.from_numpy(x).to(dev).requires_grad_(True)
+    y = mlp.net(xt)
+    assert y.shape == (N, 1) and y.dtype == torch.complex64
+    yq, cq = inr.cmlp_forward(x, params, q=inr.bf16_round)
+    y0, c0 = inr.cmlp_forward(x, params)
+    yk = y.detach().cpu().numpy()[:, 0]
+    assert rel_max(yk, yq) <= 5e-3, rel_max(yk, yq)
+    assert rel_max(yk, y0) <= 5e-2, rel_max(yk, y0)
+    gy = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    y.backward(torch.from_numpy(gy).to(dev).unsqueeze(1))
+    gq = inr.cmlp_backward(gy, params, cq)
+    net = list(mlp.net)
+    checks = [(net[0].linear.weight.grad, gq["W1"]), (net[0].linear.bias.grad, gq["b1"]),
+              (net[1].linear.weight.grad, gq["Wh"][0]), (net[1].linear.bias.grad, gq["bh"][0]),
+              (net[2].linear.weight.grad, gq["Wh"][1]), (net[2].linear.bias.grad, gq["bh"][1]),
+              (net[3].weight.grad, gq["Wo"]), (net[3].bias.grad, gq["bo"]), (xt.grad, gq["x"])]
+    for i, (got, ref) in enumerate(checks):
+        e = rel_max(got.cpu().numpy(), ref)
+        assert e <= 5e-3, (i, e)
+    for i, om in enumerate((net[0].omega_0, net[1].omega_0, net[2].omega_0)):
+        ref = gq["w1"] if i == 0 else gq["wh"][i - 1]
+        assert abs(float(om.grad) - ref) <= 5e-3 * abs(ref) + 1e-6, (i, float(om.grad), ref)
+
+
+def test_cmlp_backward_deterministic(pkg):
+    dev = torch.device("cuda")
+    mlp, _ = _mlp_from_golden(pkg, 0, dev)
+    x = torch.randn(5000, 32, device=dev) * 0.05
+    gy = torch.randn(5000, 1, dtype=torch.complex64, device=dev)
+    outs = []
+    for _ in range(2):
+        mlp.zero_grad()
+        mlp.net(x).backward(gy)
+        outs.append([p.grad.clone() for p in mlp.parameters()])
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
+
+
+def test_fused_adam_matches_torch(pkg):
+    dev = torch.device("cuda")
+    torch.manual_seed(0)
+    ps = [torch.randn(300, device=dev), torch.randn(7, 5, dtype=torch.complex64, device=dev),
+          torch.randn(1, device=dev)]
+    qs = [p.clone() for p in ps]
+    ps = [torch.nn.Parameter(p) for p in ps]
+    qs = [torch.nn.Parameter(q) for q in qs]
+    a = pkg.FusedAdam(ps, lr=3e-3)
+    b = torch.optim.Adam(qs, lr=3e-3)
+    sa = torch.optim.lr_scheduler.StepLR(a, step_size=2, gamma=0.5)
+    sb = torch.optim.lr_scheduler.StepLR(b, step_size=2, gamma=0.5)
+    for it in range(5):
+        for p, q in zip(ps, qs):
+            g = torch.randn_like(p)
+            p.grad = g.clone()
+            q.grad = g.clone()
+        a.step()
+        b.step()
+        sa.step()
+        sb.step()
+    for p, q in zip(ps, qs):
+        assert torch.allclose(p, q, rtol=1e-5, atol=1e-6)
+
+
+def test_complex_inr_model_matches_oracle_composition(pkg):
+    dev = torch.device("cuda")
+    torch.manual_seed(3)
+    m = pkg.ComplexINRModel2D(64, 64, 2, update_probe=True, probe_width=64, probe_height=64, n_levels=16,
+                              log2_hashmap_size=12, base_resolution=4, per_level_scale=1.3, first_omega_0=10.0,
+                              hidden_omega_0=1.0, trainable_omega0=True).to(dev)
+    with torch.no_grad():
+        m.xy_hash_encoder.params.uniform_(-0.1, 0.1)
+        m.probe_hash_encoder.params.uniform_(-0.1, 0.1)
+    obj, probe = m()
+    assert obj.shape == (64, 64) and probe.shape == (64, 64)
+    assert obj.dtype == torch.complex64 and torch.isfinite(torch.view_as_real(obj)).all()
+    # oracle composition: hash features -> MLP (bf16 operand rounding) -> Fourier upsample
+    levels = inr.hashgrid_levels(16, 12, 4, 1.3)
+    xy = m.xy_coords.detach().cpu().numpy().astype(np.float64)
+    feats = inr.hashgrid_encode(xy, m.xy_hash_encoder.params.detach().cpu().numpy(), levels)
+    net = list(m.object_complex_mlp.net)
+    params = {"W1": net[0].linear.weight.detach().cpu().numpy(), "b1": net[0].linear.bias.detach().cpu().numpy(),
+              "w1": float(net[0].omega_0), "Wh": [net[i].linear.weight.detach().cpu().numpy() for i in (1, 2)],
+              "bh": [net[i].linear.bias.detach().cpu().numpy() for i in (1, 2)],
+              "wh": [float(net[i].omega_0) for i in (1, 2)], "Wo": net[3].weight.detach().cpu().numpy(),
+              "bo": net[3].bias.detach().cpu().numpy()}
+    y, _ = inr.cmlp_forward(feats, params, q=inr.bf16_round)
+    ref = inr.fourier_upsample(y.reshape(32, 32), 2)
+    assert rel_max(obj.detach().cpu().numpy(), ref) <= 1e-2
+    # training step runs through every kernel and gives finite gradients
+    loss = (obj.abs() ** 2).sum() + (probe.abs() ** 2).sum()
+    loss.backward()
+    for name, p in m.named_parameters():
+        if p.requires_grad:
+            assert p.grad is not None and torch.isfinite(torch.view_as_real(p.grad) if p.is_complex()
+                                                         else p.grad).all(), name
