@@ -119,7 +119,9 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N,
  * Level l: scale s = base*per_level_scale^l - 1, r = ceil(s)+1 vertices per
  * axis, position x*s + 0.5, bilinear weights; dense index ix + iy*r when
  * r^2 (rounded up to a multiple of 8) fits in 2^log2_hashmap_size entries,
- * otherwise (ix ^ iy*2654435761) mod 2^log2_hashmap_size.
+ * otherwise (ix ^ iy*2654435761) mod 2^log2_hashmap_size.  per_level_scale
+ * is taken as float32 (as in a tiny-cuda-nn JSON config); scales are formed
+ * from it in double precision and rounded to float32.
  * ---------------------------------------------------------------------- */
 int ptycho_hashgrid_entries(int n_levels, int log2_hashmap_size, int base_resolution,
                             float per_level_scale);

@@ -54,12 +54,20 @@ def hashgrid_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scal
     return out
 
 
-def hashgrid_corners(coords, levels):
-    """For each level: (index [N,4] int64 into the level, weight [N,4])."""
+def hashgrid_corners(coords, levels, fp32_positions=False):
+    """For each level: (index [N,4] int64 into the level, weight [N,4]).
+
+    ``fp32_positions`` forms the grid position as a single-rounded float32
+    ``x * float32(scale) + 0.5`` (a fused multiply-add), the arithmetic the
+    CUDA kernel uses; otherwise positions are FP64."""
     x = np.asarray(coords, dtype=np.float64)
     res_all = []
     for (scale, res, n, off, dense) in levels:
-        p = x * scale + 0.5
+        if fp32_positions:
+            s32 = np.float64(np.float32(scale))
+            p = (np.float32(x).astype(np.float64) * s32 + 0.5).astype(np.float32).astype(np.float64)
+        else:
+            p = x * scale + 0.5
         g = np.floor(p)
         f = p - g
         gi = g.astype(np.int64)
@@ -82,12 +90,12 @@ def hashgrid_corners(coords, levels):
     return res_all
 
 
-def hashgrid_encode(coords, table, levels, F=2):
+def hashgrid_encode(coords, table, levels, F=2, fp32_positions=False):
     """Features [N, L*F]: per level the bilinear blend of the 4 corner entries.
 
     ``table`` is flat: level l occupies entries [off_l, off_l + n_l), F floats each."""
     tab = np.asarray(table, dtype=np.float64).reshape(-1, F)
-    corners = hashgrid_corners(coords, levels)
+    corners = hashgrid_corners(coords, levels, fp32_positions)
     N = np.asarray(coords).shape[0]
     out = np.zeros((N, len(levels) * F))
     for l, ((scale, res, n, off, dense), (idx, w)) in enumerate(zip(levels, corners)):
@@ -95,10 +103,10 @@ def hashgrid_encode(coords, table, levels, F=2):
     return out
 
 
-def hashgrid_backward(coords, dfeat, levels, n_entries, F=2):
+def hashgrid_backward(coords, dfeat, levels, n_entries, F=2, fp32_positions=False):
     """d table (flat, [n_entries * F]) from d features [N, L*F]."""
     g = np.zeros((n_entries, F))
-    corners = hashgrid_corners(coords, levels)
+    corners = hashgrid_corners(coords, levels, fp32_positions)
     for l, ((scale, res, n, off, dense), (idx, w)) in enumerate(zip(levels, corners)):
         d = np.asarray(dfeat, dtype=np.float64)[:, l * F:(l + 1) * F]
         for k in range(4):
