@@ -331,6 +331,109 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_time_to_residual(args):
+    """Time-to-residual on workload c2 (1024^2 canvas, 128^2 probe, 28x28 raster,
+    smooth_L1, batch 10): the pixel grid (object and probe as plain parameters,
+    fused kernels, Adam lr 1e-2) trains for --pg-epochs epochs and sets the
+    target = 1.1 x its final data residual R = sum (sqrt(I) - sqrt(Imeas))^2 /
+    sum Imeas (FP64 over the whole stack).  Then the INR built on the
+    hand-written kernels and the reference INR (models/complex_inr.py and the
+    per-frame Recovery.py loop in torch with torch.fft; tiny-cuda-nn replaced by
+    a torch HashGrid restatement because it cannot be installed) each train
+    until R <= target or their wall-time cap.  R is evaluated once per epoch,
+    outside the timed wall time."""
+    dev = torch.device("cuda")
+    pkg = importlib.import_module(PKG)
+    rec = importlib.import_module(PKG + ".recovery")
+    from oracle import torch_inr
+    work = pkg.synth.make_workload("c2", device=dev)
+    stack = torch.from_numpy(work["Imeas"]).to(dev)
+    tl = pkg.make_windows(work["tlY"], work["tlX"], dev)
+    F, M = stack.shape[0], stack.shape[1]
+    P0 = torch.from_numpy(work["probe"].astype(np.complex64)).to(dev) * float(np.sqrt(M * M))
+    pls = torch_inr.per_level_scale_for(512, 16, 16)
+    out = {"metric": "time-to-residual (pixel-grid x1.1)", "workload": WORKLOADS_DESC["c2"], "frames": F}
+
+    def timed(trainer, max_epochs, max_s, target):
+        hist, t_train, reached = [], 0.0, None
+        for ep in range(max_epochs):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            trainer.epoch()
+            torch.cuda.synchronize()
+            t_train += time.perf_counter() - t0
+            r = trainer.residual()
+            hist.append((ep + 1, round(t_train, 3), r))
+            if target is not None and r <= target and reached is None:
+                reached = (ep + 1, t_train, r)
+                break
+            if t_train > max_s:
+                break
+        return hist, reached, t_train
+
+    pg = rec.PixelGrid((1024, 1024), (M, M), probe_init=P0).to(dev)
+    tpg = rec.Trainer(pg, stack, tl, "smooth_L1_loss", 10, 1e-2)
+    hist, _, t_pg = timed(tpg, args.pg_epochs, 1e9, None)
+    r_pg = hist[-1][2]
+    target = 1.1 * r_pg
+    out["pixel_grid"] = {"epochs": len(hist), "seconds": round(t_pg, 3), "residual": r_pg,
+                         "history": hist[:: max(1, len(hist) // 10)]}
+    out["target_residual"] = target
+    cfg = dict(model_type="inr", downsample_factor=2, n_levels=16, log2_hashmap_size=18, base_resolution=16,
+               per_level_scale=pls, first_omega_0=10.0, hidden_omega_0=1.0, trainable_omega0=True,
+               use_residual=True, init_type="initProbe")
+    model = rec.build_model(cfg, 1024, (M, M), P0, dev)
+    tin = rec.Trainer(model, stack, tl, "smooth_L1_loss", 10, 1e-3)
+    hist, reached, t_in = timed(tin, args.inr_epochs, args.inr_cap_s, target)
+    out["inr_b200_kernels"] = {"reached": reached is not None, "seconds_to_target": reached[1] if reached else None,
+                               "epochs_to_target": reached[0] if reached else None,
+                               "seconds": round(t_in, 3), "best_residual": min(h[2] for h in hist),
+                               "ms_per_minibatch": 1e3 * t_in / (len(hist) * -(-F // 10)),
+                               "history": hist[:: max(1, len(hist) // 10)]}
+
+    class RefTrainer:  # the reference loop, per frame, on this GPU
+        def __init__(self):
+            self.model = torch_inr.RefINR(1024, 2, M, 16, 18, 16, pls, 10.0, 1.0, probe_initial=P0).to(dev)
+            self.opt = torch.optim.Adam([p for p in self.model.parameters() if p.requires_grad], lr=1e-3)
+            self.mmf = stack.permute(1, 2, 0).contiguous()
+            self.rng = np.random.default_rng(0)
+
+        def epoch(self):
+            perm = self.rng.permutation(F)
+            for s0 in range(0, F, 10):
+                torch_inr.ref_minibatch(self.model, self.opt, self.mmf, work["tlY"], work["tlX"],
+                                        perm[s0:s0 + 10], "smooth_L1_loss")
+
+        @torch.no_grad()
+        def residual(self):
+            obj, probe = self.model()
+            probe = rec.center_and_normalize_probe(probe)
+            num = den = 0.0
+            for s0 in range(0, F, 256):
+                ids = torch.arange(s0, min(F, s0 + 256), device=dev, dtype=torch.int32)
+                I = pkg.forward_intensity(obj.to(torch.complex64), probe.to(torch.complex64), tl, batch=ids).double()
+                Im = stack[ids.long()].double()
+                num += float(((I.sqrt() - Im.sqrt()) ** 2).sum())
+                den += float(Im.sum())
+            return num / den
+
+    hist, reached, t_ref = timed(RefTrainer(), args.inr_epochs, args.ref_cap_s, target)
+    out["inr_reference_torch"] = {"reached": reached is not None,
+                                  "seconds_to_target": reached[1] if reached else None,
+                                  "epochs_to_target": reached[0] if reached else None,
+                                  "seconds": round(t_ref, 3), "best_residual": min(h[2] for h in hist),
+                                  "ms_per_minibatch": 1e3 * t_ref / (len(hist) * -(-F // 10)),
+                                  "history": hist,
+                                  "note": "reference ComplexINRModel2D/ComplexMLP and per-frame loop in torch "
+                                          "(torch.fft); tiny-cuda-nn replaced by a torch HashGrid restatement"}
+    print(json.dumps(out), flush=True)
+
+
+WORKLOADS_DESC = {"c2": "c2: 1024^2 canvas, 128^2 probe, 28x28 raster (784 frames), smooth_L1, batch 10; INR "
+                        "16 levels x 2, log2 T 18, base 16, finest 512, 512^2 object grid (ds 2), MLP 64x2, "
+                        "omega 10/1, probe initProbe + residual"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -341,7 +444,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-batch", type=int, default=0)
+    ap.add_argument("--time-to-residual", action="store_true")
+    ap.add_argument("--pg-epochs", type=int, default=100)
+    ap.add_argument("--inr-epochs", type=int, default=2000)
+    ap.add_argument("--inr-cap-s", type=float, default=120.0)
+    ap.add_argument("--ref-cap-s", type=float, default=180.0)
     args = ap.parse_args()
+    if args.time_to_residual:
+        run_time_to_residual(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -41,6 +41,8 @@ SIGNATURES = {
     "ptycho_cmlp_backward": (_c_int, [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _c_size, _vp, _vp]),
     "ptycho_adam_step": (_c_int, [_pp, _pp, _pp, _pp, ctypes.POINTER(_c_ll), _c_int, _c_int, _c_float, _c_float,
                                   _c_float, _c_float, _vp]),
+    "ptycho_adam_step_dev": (_c_int, [_pp, _pp, _pp, _pp, ctypes.POINTER(_c_ll), _c_int, _vp, _vp, _c_float,
+                                      _c_float, _c_float, _vp]),
     "ptycho_fwd_adj_noalloc": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp,
                                         _c_int, _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _vp]),
 }

@@ -22,10 +22,55 @@ def _real(t):
 
 
 class FusedAdam(torch.optim.Optimizer):
-    def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, weight_decay=0.0, amsgrad=False):
+    """``capturable=True`` keeps each group's step counter and learning rate in
+    device memory (``ptycho_adam_step_dev``) so ``step()`` can be captured in a
+    CUDA graph; call ``sync_lr()`` after changing a group's lr (e.g. after
+    ``StepLR.step()``).  In that mode every parameter of a group must receive a
+    gradient at every step (they share one counter)."""
+
+    def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, weight_decay=0.0, amsgrad=False,
+                 capturable=False):
         if weight_decay != 0.0 or amsgrad:
             raise NotImplementedError("weight_decay and amsgrad are not supported")
         super().__init__(params, dict(lr=lr, betas=betas, eps=eps))
+        self.capturable = capturable
+        self._dev = []
+        if capturable:
+            for g in self.param_groups:
+                dev = g["params"][0].device
+                self._dev.append({"step": torch.zeros(1, dtype=torch.int32, device=dev),
+                                  "lr": torch.tensor([g["lr"]], dtype=torch.float32, device=dev)})
+
+    def sync_lr(self):
+        """Copy each group's current lr into its device copy (capturable mode)."""
+        for g, d in zip(self.param_groups, self._dev):
+            d["lr"].fill_(float(g["lr"]))
+
+    @torch.no_grad()
+    def _step_capturable(self):
+        L = _lib.lib()
+        for group, d in zip(self.param_groups, self._dev):
+            ps = [p for p in group["params"] if p.grad is not None]
+            if not ps:
+                continue
+            if len(ps) > 48:
+                raise ValueError("capturable FusedAdam handles at most 48 tensors per group")
+            for p in ps:
+                st = self.state[p]
+                if not st:
+                    st["exp_avg"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
+                    st["exp_avg_sq"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
+            grads = [_real(p.grad).contiguous() for p in ps]
+            n = len(ps)
+            arr = lambda xs: ctypes.cast((ctypes.c_void_p * n)(*xs), ctypes.POINTER(ctypes.c_void_p))  # noqa: E731
+            N = (ctypes.c_longlong * n)(*[_real(p).numel() for p in ps])
+            b1, b2 = group["betas"]
+            _lib.check(L.ptycho_adam_step_dev(
+                arr([_real(p).data_ptr() for p in ps]), arr([g.data_ptr() for g in grads]),
+                arr([_real(self.state[p]["exp_avg"]).data_ptr() for p in ps]),
+                arr([_real(self.state[p]["exp_avg_sq"]).data_ptr() for p in ps]), N, n, d["step"].data_ptr(),
+                d["lr"].data_ptr(), float(b1), float(b2), float(group["eps"]),
+                torch.cuda.current_stream(ps[0].device).cuda_stream), "ptycho_adam_step_dev")
 
     @torch.no_grad()
     def step(self, closure=None):
@@ -33,6 +78,9 @@ class FusedAdam(torch.optim.Optimizer):
         if closure is not None:
             with torch.enable_grad():
                 loss = closure()
+        if self.capturable:
+            self._step_capturable()
+            return loss
         L = _lib.lib()
         for group in self.param_groups:
             ps = [p for p in group["params"] if p.grad is not None]

@@ -42,9 +42,79 @@ __global__ void __launch_bounds__(256) k_adam(const AdamList L, long long total,
   }
 }
 
+// capturable form: step counter and learning rate live in device memory, so a
+// CUDA graph that replays the step stays correct; k_adam_tick advances the
+// counter, every block derives the bias corrections from it
+__global__ void k_adam_tick(int* step) { step[0] += 1; }
+
+__global__ void __launch_bounds__(256) k_adam_dev(const AdamList L, long long total, const int* __restrict__ step,
+                                                  const float* __restrict__ lr, float b1, float b2, float eps) {
+  __shared__ float sc[2];
+  if (threadIdx.x == 0) {
+    const double t = (double)step[0];
+    const double bc1 = 1.0 - pow((double)b1, t), bc2 = 1.0 - pow((double)b2, t);
+    sc[0] = (float)((double)lr[0] / bc1);
+    sc[1] = (float)(1.0 / sqrt(bc2));
+  }
+  __syncthreads();
+  const float lr_bc1 = sc[0], inv_sqrt_bc2 = sc[1];
+  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < total; i += (long long)gridDim.x * 256) {
+    int k = 0;
+    while (L.end[k] <= i) ++k;
+    const long long j = i - (k ? L.end[k - 1] : 0);
+    const float g = L.g[k][j];
+    float m = L.m[k][j], v = L.v[k][j];
+    m = fmaf(1.0f - b1, g - m, m);
+    v = fmaf(1.0f - b2, g * g, b2 * v);
+    const float denom = sqrtf(v) * inv_sqrt_bc2 + eps;
+    L.p[k][j] -= lr_bc1 * (m / denom);
+    L.m[k][j] = m;
+    L.v[k][j] = v;
+  }
+}
+
+static int make_list(float* const* params, const float* const* grads, float* const* exp_avg,
+                     float* const* exp_avg_sq, const long long* numels, int n_tensors, AdamList* L,
+                     long long* total) {
+  if (n_tensors < 0 || n_tensors > kAdamMaxTensors) return PTYCHO_ERR_INVALID_ARG;
+  if (n_tensors > 0 && (!params || !grads || !exp_avg || !exp_avg_sq || !numels)) return PTYCHO_ERR_INVALID_ARG;
+  *total = 0;
+  for (int k = 0; k < n_tensors; ++k) {
+    if (numels[k] < 0 || (numels[k] > 0 && (!params[k] || !grads[k] || !exp_avg[k] || !exp_avg_sq[k])))
+      return PTYCHO_ERR_INVALID_ARG;
+    L->p[k] = params[k];
+    L->g[k] = grads[k];
+    L->m[k] = exp_avg[k];
+    L->v[k] = exp_avg_sq[k];
+    *total += numels[k];
+    L->end[k] = *total;
+  }
+  L->n = n_tensors;
+  return PTYCHO_OK;
+}
+
 }  // namespace pty
 
 using namespace pty;
+
+extern "C" int ptycho_adam_step_dev(float* const* params, const float* const* grads, float* const* exp_avg,
+                                    float* const* exp_avg_sq, const long long* numels, int n_tensors,
+                                    int32_t* step, const float* lr, float beta1, float beta2, float eps,
+                                    ptycho_stream_t stream) {
+  if (!step || !lr) return PTYCHO_ERR_INVALID_ARG;
+  AdamList L{};
+  long long total = 0;
+  int st = make_list(params, grads, exp_avg, exp_avg_sq, numels, n_tensors, &L, &total);
+  if (st) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  k_adam_tick<<<1, 1, 0, s>>>(step);
+  if (total > 0) {
+    const long long blocks = (total + 255) / 256;
+    const int grid = (int)(blocks < 148 * 16 ? blocks : 148 * 16);
+    k_adam_dev<<<grid, 256, 0, s>>>(L, total, step, lr, beta1, beta2, eps);
+  }
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
 
 extern "C" int ptycho_adam_step(float* const* params, const float* const* grads, float* const* exp_avg,
                                 float* const* exp_avg_sq, const long long* numels, int n_tensors, int step,

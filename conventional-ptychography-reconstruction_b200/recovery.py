@@ -131,12 +131,13 @@ def center_and_normalize_probe(P: torch.Tensor) -> torch.Tensor:
     with torch.no_grad():
         a = P.detach().abs() ** 2
         tot = a.sum()
-        MN = torch.tensor([M, N], device=dev, dtype=a.dtype)
-        com = torch.stack((a.sum(1).cumsum(0).mean(), a.sum(0).cumsum(0).mean()))
-        cp = torch.trunc(MN / 2 - MN * com / torch.where(tot == 0, torch.ones_like(tot), tot) + 1)
-        cp = torch.where(tot == 0, torch.zeros_like(cp), cp).long()
-        iy = (torch.arange(M, device=dev) + cp[0]) % M
-        ix = (torch.arange(N, device=dev) + cp[1]) % N
+        safe = torch.where(tot == 0, torch.ones_like(tot), tot)
+        cy = torch.trunc(M / 2 - M * a.sum(1).cumsum(0).mean() / safe + 1)
+        cx = torch.trunc(N / 2 - N * a.sum(0).cumsum(0).mean() / safe + 1)
+        cy = torch.where(tot == 0, torch.zeros_like(cy), cy).long()
+        cx = torch.where(tot == 0, torch.zeros_like(cx), cx).long()
+        iy = (torch.arange(M, device=dev) + cy) % M
+        ix = (torch.arange(N, device=dev) + cx) % N
     P = P[iy][:, ix]  # == torch.roll(P, (-cp0, -cp1), (0, 1))
     e = (P.abs() ** 2).sum()
     scale = torch.where(e > 0, torch.sqrt(float(M * N) / torch.where(e > 0, e, torch.ones_like(e))),
@@ -156,7 +157,7 @@ class Trainer:
     """The reference training loop on resident data (one object per run)."""
 
     def __init__(self, model, stack, tl, loss_type, batch_size, lr, lr_decay_step=10000, lr_decay_gamma=0.1,
-                 sparsity_weight=0.0, seed=0):
+                 sparsity_weight=0.0, seed=0, use_graph=True):
         self.model = model
         self.stack = stack  # [F, M, M] float32, device
         self.tl = tl        # [F, 2] int32, device
@@ -164,10 +165,67 @@ class Trainer:
         self.loss_type = loss_type
         self.batch_size = int(batch_size)
         self.sparsity_weight = float(sparsity_weight)
-        self.opt = FusedAdam([p for p in model.parameters() if p.requires_grad], lr=lr)
+        self.opt = FusedAdam([p for p in model.parameters() if p.requires_grad], lr=lr, capturable=use_graph)
         self.sched = torch.optim.lr_scheduler.StepLR(self.opt, step_size=lr_decay_step, gamma=lr_decay_gamma)
         self.gen = torch.Generator(device=stack.device).manual_seed(seed)
         self.last_loss = None
+        self.use_graph = use_graph
+        self._graphs = {}  # minibatch length -> (graph, static batch buffer, static loss)
+        self._pool = None
+
+    def _graph_for(self, n: int):
+        """Capture the whole minibatch step (model forward, fused loss, backward,
+        Adam) for minibatches of length n; the frame ids live in a static buffer."""
+        ent = self._graphs.get(n)
+        if ent is not None:
+            return ent
+        dev = self.stack.device
+        buf = torch.arange(n, dtype=torch.int32, device=dev)
+        # warm-up outside capture (CSR, workspaces, FFT plans, kernel attributes);
+        # parameters and optimizer state are restored afterwards
+        params = [p for p in self.model.parameters()]
+        saved = [p.detach().clone() for p in params]
+        saved_opt = {k: (v["exp_avg"].clone(), v["exp_avg_sq"].clone()) for k, v in self.opt.state.items()
+                     if "exp_avg" in v}
+        saved_dev = [(d["step"].clone(), d["lr"].clone()) for d in self.opt._dev]
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            for _ in range(2):
+                self.step(buf)
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        with torch.no_grad():
+            for p, v in zip(params, saved):
+                p.copy_(v)
+            for k, v in self.opt.state.items():
+                if "exp_avg" in v:
+                    if k in saved_opt:
+                        v["exp_avg"].copy_(saved_opt[k][0])
+                        v["exp_avg_sq"].copy_(saved_opt[k][1])
+                    else:
+                        v["exp_avg"].zero_()
+                        v["exp_avg_sq"].zero_()
+            for d, (st, lr) in zip(self.opt._dev, saved_dev):
+                d["step"].copy_(st)
+                d["lr"].copy_(lr)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, pool=self._pool):
+            loss = self.step(buf)
+        self._pool = g.pool()
+        ent = (g, buf, loss)
+        self._graphs[n] = ent
+        return ent
+
+    def run(self, batch_ids: torch.Tensor) -> torch.Tensor:
+        """One minibatch: replay of the captured step (or an eager step)."""
+        if not self.use_graph:
+            return self.step(batch_ids)
+        g, buf, loss = self._graph_for(int(batch_ids.numel()))
+        buf.copy_(batch_ids)
+        g.replay()
+        self.last_loss = loss
+        return loss
 
     def step(self, batch_ids: torch.Tensor) -> torch.Tensor:
         self.opt.zero_grad(set_to_none=True)
@@ -187,8 +245,10 @@ class Trainer:
     def epoch(self):
         perm = torch.randperm(self.F, device=self.stack.device, generator=self.gen).to(torch.int32)
         for s in range(0, self.F, self.batch_size):
-            self.step(perm[s:s + self.batch_size])
+            self.run(perm[s:s + self.batch_size])
         self.sched.step()
+        if self.use_graph:
+            self.opt.sync_lr()
 
     @torch.no_grad()
     def current(self):

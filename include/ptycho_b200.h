@@ -190,6 +190,15 @@ int ptycho_adam_step(float* const* params, const float* const* grads, float* con
                      float* const* exp_avg_sq, const long long* numels, int n_tensors, int step,
                      float lr, float beta1, float beta2, float eps, ptycho_stream_t stream);
 
+/* The same step with the step counter (device int32, incremented by the
+ * call before use) and the learning rate (device float32) in device memory,
+ * so the call can be captured once in a CUDA graph and replayed every step
+ * (the torch.optim.Adam(capturable=True) arrangement). */
+int ptycho_adam_step_dev(float* const* params, const float* const* grads, float* const* exp_avg,
+                         float* const* exp_avg_sq, const long long* numels, int n_tensors,
+                         int32_t* step, const float* lr, float beta1, float beta2, float eps,
+                         ptycho_stream_t stream);
+
 /* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
