@@ -44,18 +44,20 @@ constexpr int S_W2 = S_W1 + 2048;   // Wr2 [64][64]          LBO 1024
 constexpr int S_W3 = S_W2 + 8192;   // Wr3 [64][64]
 constexpr int S_WO = S_W3 + 8192;   // Wor [16][64] (rows 0,1 used), LBO 256
 constexpr int kWBytes = S_WO + 2048;  // 20480
-constexpr int S_X = kWBytes;        // 6 groups: x (4), ones, zeros
+constexpr int S_PAR = kWBytes;      // fp32 biases and omegas
+constexpr int S_BAR = S_PAR + 1024;
+constexpr int S_TMEM = S_BAR + 16;
+constexpr int S_RED = S_TMEM + 16;
+constexpr int S_X = S_RED + 64;     // 6 groups: x (4), ones, zeros
 constexpr int S_H = S_X + 6 * GRP;  // 18 groups: h2 (8), h1 (8), ones, zeros
 constexpr int S_H3 = S_H + 18 * GRP;  // 10 groups: h3 (8), ones, zeros
 constexpr int S_GY = S_H3 + 10 * GRP;  // 2 groups: (G_yr, G_yi, 0, ...), zeros
 constexpr int S_GZ1 = S_GY + 2 * GRP;  // 4 groups: G_z1
 constexpr int S_GZ = S_GZ1 + 4 * GRP;  // 16 groups: G_z3 (8), G_z2 (8)
 constexpr int S_ACT_END = S_GZ + 16 * GRP;
-constexpr int S_PAR = S_ACT_END;    // fp32 biases and omegas
-constexpr int S_BAR = S_PAR + 1024;
-constexpr int S_TMEM = S_BAR + 16;
-constexpr int S_RED = S_TMEM + 16;
-constexpr int kSmem = S_RED + 64;
+constexpr int kSmemBwd = S_ACT_END;  // 136288 bytes: one CTA per SM
+constexpr int kSmemFwd = S_GY;       // 91200 bytes: the forward needs x, h, h3 only -> two CTAs per SM
+
 // every MMA footprint used below stays inside [0, S_ACT_END)
 static_assert(S_GY + 16 * GRP <= S_ACT_END, "output-grad A footprint");
 static_assert(S_GZ1 + 16 * GRP <= S_ACT_END, "layer-1 grad A footprint");
@@ -153,7 +155,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
   const uint32_t sbase = tc::smem_addr(sm);
 
   // -- set-up: zero activations, copy weights and parameters, ones columns ----
-  for (int i = t; i < (S_ACT_END - S_X) / 16; i += kThreads)
+  constexpr int kActEnd = BWD ? S_ACT_END : S_GY;
+  for (int i = t; i < (kActEnd - S_X) / 16; i += kThreads)
     reinterpret_cast<uint4*>(sm + S_X)[i] = make_uint4(0u, 0u, 0u, 0u);
   for (int i = t; i < kWBytes / 16; i += kThreads)
     reinterpret_cast<uint4*>(sm)[i] = __ldg(reinterpret_cast<const uint4*>(a.packed) + i);
@@ -476,7 +479,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
 // sum the CTA partials in CTA order and fold the real-form blocks
 __global__ void __launch_bounds__(256) k_cmlp_reduce(const float* __restrict__ part, int nparts,
                                                      float* __restrict__ grad) {
-  const int e = blockIdx.x * 256 + threadIdx.x;
+  const int e = blockIdx.x * 8 + (threadIdx.x >> 5);  // one warp per output
+  const int lane = threadIdx.x & 31;
   if (e >= kGradFloats) return;
   // each output is a (sign-weighted) sum of at most two raw entries
   int i0 = -1, i1 = -1;
@@ -525,16 +529,19 @@ __global__ void __launch_bounds__(256) k_cmlp_reduce(const float* __restrict__ p
   } else if (e >= G_BO) {
     i0 = R_BO + (e - G_BO);
   }
+  // lane j sums partials j, j+32, ... in order; then a fixed xor tree
   float acc = 0.f;
   if (i0 >= 0) {
-    for (int p = 0; p < nparts; ++p) {
+    for (int p = lane; p < nparts; p += 32) {
       const float* P = part + size_t(p) * kPartFloats;
       float v = P[i0];
       if (i1 >= 0) v = fmaf(s1, P[i1], v);
       acc += v;
     }
   }
-  grad[e] = acc;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) grad[e] = acc;
 }
 
 // pack torch-layout parameters into the kernel's bf16 operand blob + fp32 block
@@ -588,16 +595,18 @@ __global__ void __launch_bounds__(256) k_cmlp_pack(const PackArgs p) {
 template <bool BWD>
 static int launch(const Args& a, cudaStream_t s, int* grid_out) {
   auto kern = k_cmlp<BWD>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
+  constexpr int smem = BWD ? kSmemBwd : kSmemFwd;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return PTYCHO_ERR_LAUNCH;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (a.N + 127) / 128;
-  const int grid = ntiles < nsm ? ntiles : nsm;
+  const int per_sm = BWD ? 1 : 2;  // TMEM: 512 columns (backward) or 2 x 256 (forward) per SM
+  const int grid = ntiles < nsm * per_sm ? ntiles : nsm * per_sm;
   if (grid_out) *grid_out = grid;
   if (grid == 0) return PTYCHO_OK;
-  kern<<<grid, kThreads, kSmem, s>>>(a);
+  kern<<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
@@ -666,7 +675,7 @@ int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, in
   int grid = 0;
   int st = cm::launch<true>(a, s, &grid);
   if (st) return st;
-  cm::k_cmlp_reduce<<<(cm::kGradFloats + 255) / 256, 256, 0, s>>>(static_cast<const float*>(workspace), grid,
+  cm::k_cmlp_reduce<<<(cm::kGradFloats + 7) / 8, 256, 0, s>>>(static_cast<const float*>(workspace), grid,
                                                                   grad);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }

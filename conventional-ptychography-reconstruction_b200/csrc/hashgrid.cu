@@ -68,28 +68,33 @@ PTY_DEVI int corner_entry(const LevelTable& L, int l, int cx, int cy) {
   return L.offset[l] + int(e % uint32_t(L.n[l]));
 }
 
-// one thread per (coordinate, level): 4 corner gathers of float2, bilinear blend
+// one thread per coordinate, all levels: adjacent threads hold adjacent
+// coordinates, so each level's corner gathers of a warp fall on neighbouring
+// cells, and a thread writes its n_levels x 2 features contiguously
 __global__ void __launch_bounds__(256) k_hash_fwd(const float2* __restrict__ coords, int N,
                                                   const float2* __restrict__ table, const LevelTable L,
                                                   float2* __restrict__ feat) {
-  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
-  if (i >= (long long)N * L.levels) return;
-  const int n = int(i / L.levels), l = int(i - (long long)n * L.levels);
+  const int n = blockIdx.x * 256 + threadIdx.x;
+  if (n >= N) return;
   const float2 x = __ldg(coords + n);
-  const float s = L.scale[l];
-  const float px = fmaf(x.x, s, 0.5f), py = fmaf(x.y, s, 0.5f);
-  const float gx = floorf(px), gy = floorf(py);
-  const float fx = px - gx, fy = py - gy;
-  const int ix = int(gx), iy = int(gy);
-  const float2 t00 = __ldg(table + corner_entry(L, l, ix, iy));
-  const float2 t10 = __ldg(table + corner_entry(L, l, ix + 1, iy));
-  const float2 t01 = __ldg(table + corner_entry(L, l, ix, iy + 1));
-  const float2 t11 = __ldg(table + corner_entry(L, l, ix + 1, iy + 1));
-  const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
-  float2 o;
-  o.x = fmaf(w11, t11.x, fmaf(w01, t01.x, fmaf(w10, t10.x, w00 * t00.x)));
-  o.y = fmaf(w11, t11.y, fmaf(w01, t01.y, fmaf(w10, t10.y, w00 * t00.y)));
-  feat[(long long)n * L.levels + l] = o;
+  float2* out = feat + (long long)n * L.levels;
+#pragma unroll 4
+  for (int l = 0; l < L.levels; ++l) {
+    const float s = L.scale[l];
+    const float px = fmaf(x.x, s, 0.5f), py = fmaf(x.y, s, 0.5f);
+    const float gx = floorf(px), gy = floorf(py);
+    const float fx = px - gx, fy = py - gy;
+    const int ix = int(gx), iy = int(gy);
+    const float2 t00 = __ldg(table + corner_entry(L, l, ix, iy));
+    const float2 t10 = __ldg(table + corner_entry(L, l, ix + 1, iy));
+    const float2 t01 = __ldg(table + corner_entry(L, l, ix, iy + 1));
+    const float2 t11 = __ldg(table + corner_entry(L, l, ix + 1, iy + 1));
+    const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
+    float2 o;
+    o.x = fmaf(w11, t11.x, fmaf(w01, t01.x, fmaf(w10, t10.x, w00 * t00.x)));
+    o.y = fmaf(w11, t11.y, fmaf(w01, t01.y, fmaf(w10, t10.y, w00 * t00.y)));
+    out[l] = o;
+  }
 }
 
 // contributions: for coordinate n, level l, corner k -> key = entry,
@@ -207,8 +212,7 @@ int ptycho_hashgrid_forward(const float* coords, int N, const float* table, int 
   if (!pty_aligned(coords, 8) || !pty_aligned(table, 8) || !pty_aligned(features, 8))
     return PTYCHO_ERR_MISALIGNED;
   if (N == 0) return PTYCHO_OK;
-  const long long work = (long long)N * n_levels;
-  k_hash_fwd<<<(unsigned)((work + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+  k_hash_fwd<<<(unsigned)((N + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<const float2*>(coords), N, reinterpret_cast<const float2*>(table), L,
       reinterpret_cast<float2*>(features));
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
