@@ -7,6 +7,7 @@ The directory name is not a Python identifier; import it with
 """
 from . import _lib, optics, synth
 from . import adam, cmlp, complex_inr, hashgrid
+from ._lib import PtychoError
 from .adam import FusedAdam
 from .complex_inr import ComplexINRModel2D
 from .hashgrid import Encoding
@@ -14,7 +15,7 @@ from .optics import (LOSS_CODES, forward_imaging_model, forward_intensity, forwa
                      fused_loss, fwd_adj_raw, make_windows, check_windows, read_status,
                      scan_positions_to_pixels)
 
-__all__ = ["FusedAdam", "ComplexINRModel2D", "Encoding", "LOSS_CODES", "forward_imaging_model", "forward_intensity", "forward_intensity_batched",
+__all__ = ["PtychoError", "FusedAdam", "ComplexINRModel2D", "Encoding", "LOSS_CODES", "forward_imaging_model", "forward_intensity", "forward_intensity_batched",
            "fused_loss", "fwd_adj_raw", "make_windows", "check_windows", "read_status",
            "scan_positions_to_pixels", "lib"]
 

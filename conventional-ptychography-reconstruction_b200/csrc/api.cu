@@ -29,7 +29,7 @@ static WsLayout ws_layout(int M, int B) {
   return L;
 }
 
-static bool supported_probe(int M, int N) { return M == N && (M == 64 || M == 128); }
+static bool supported_probe(int M, int N) { return M == N && (M == 64 || M == 128 || M == 256); }
 
 static int check_common(const float* O, int H, int W, const float* P, int M, int N, const int32_t* tl,
                         int F, const int32_t* batch, int B) {
@@ -43,7 +43,9 @@ static int check_common(const float* O, int H, int W, const float* P, int M, int
 }
 
 static int launch_fused(int M, int mode, int loss, const FusedArgs& a, cudaStream_t s) {
-  return M == 64 ? launch_fused_64(mode, loss, a, s) : launch_fused_128(mode, loss, a, s);
+  if (M == 64) return launch_fused_64(mode, loss, a, s);
+  if (M == 128) return launch_fused_128(mode, loss, a, s);
+  return launch_fused_256(mode, loss, a, s);
 }
 
 static FusedArgs make_args(const float* O, int H, int W, const float* P, const int32_t* tl,
@@ -110,6 +112,7 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   int st = check_common(O, H, W, P, M, N, tl, F, batch, B);
   if (st) return st;
   if (loss_type < 0 || loss_type > 3) return PTYCHO_ERR_INVALID_ARG;
+  if (M == 256 && loss_type == PTYCHO_LOSS_FD) return PTYCHO_ERR_UNSUPPORTED_SIZE;
   if (B > 0 && !Imeas) return PTYCHO_ERR_INVALID_ARG;
   if (!pty_aligned(Imeas, 16)) return PTYCHO_ERR_MISALIGNED;
   if ((dO && !pty_aligned(dO, 8)) || (dP && !pty_aligned(dP, 8))) return PTYCHO_ERR_MISALIGNED;

@@ -29,6 +29,8 @@ struct PassDesc {
   int tbit[10];  // thread bit j -> position bit
   int nbx, lox;  // x DIF stage of this pass: digit width (0 = none), lowest bit
   int nby, loy;  // y DIF stage
+  int nr = 0;          // cluster-rank bits (patterns split over a CTA cluster)
+  int rbit[2] = {0, 0};  // rank bit j -> position bit
 };
 
 struct FreqMap {
@@ -59,17 +61,33 @@ struct Plan<128> {
   static constexpr FreqMap F = {{4, 5, 6, 0, 1, 2, 3}, {3, 4, 5, 6, 1, 2, 0}};
 };
 
+// M = 256: a cluster of 4 CTAs per pattern (512 threads x 32 values each);
+// x = 16 * 16, y = 2 * 2 * 16 * 4 in four passes.  Passes 1-2 split rows by
+// y bits 4,5 across the cluster, passes 3-4 by y bits 6,7; the exchange
+// between passes 2 and 3 goes through distributed shared memory.
+template <>
+struct Plan<256> {
+  static constexpr int LOGM = 8, NT = 512, E = 32, CLUSTER = 4, MIN_BLOCKS = 1;
+  static constexpr PassDesc P1 = {5, {4, 5, 6, 7, 15}, 9, {0, 1, 2, 3, 8, 9, 10, 11, 14}, 4, 4, 1, 7, 2, {12, 13}};
+  static constexpr PassDesc P2 = {5, {0, 1, 2, 3, 14}, 9, {4, 5, 6, 7, 9, 8, 10, 11, 15}, 4, 0, 1, 6, 2, {12, 13}};
+  static constexpr PassDesc P3 = {5, {10, 11, 12, 13, 0}, 9, {1, 2, 3, 7, 9, 4, 5, 6, 8}, 0, 0, 4, 2, 2, {14, 15}};
+  static constexpr PassDesc P4 = {5, {8, 9, 1, 2, 3}, 9, {0, 4, 5, 6, 7, 10, 11, 12, 13}, 0, 0, 2, 0, 2, {14, 15}};
+  static constexpr FreqMap F = {{4, 5, 6, 7, 0, 1, 2, 3}, {6, 7, 2, 3, 4, 5, 1, 0}};
+};
+
 // column swizzle: bits 5 (and 6) of the column are XOR-ed onto bits 1 (and 2)
 template <int M>
 __host__ __device__ constexpr int swz(int px) {
-  return px ^ ((px >> 4) & Plan<M>::SWZ);
+  if constexpr (M == 256) return px ^ (((px >> 4) & 0xF) << 1);
+  else return px ^ ((px >> 4) & Plan<M>::SWZ);
 }
 
 template <int M, int PASS>
 __host__ __device__ constexpr PassDesc desc() {
   if constexpr (PASS == 1) return Plan<M>::P1;
   else if constexpr (PASS == 2) return Plan<M>::P2;
-  else return Plan<M>::P3;
+  else if constexpr (PASS == 3) return Plan<M>::P3;
+  else return Plan<M>::P4;
 }
 
 // compile-time x / y offset of element e within a pass
@@ -126,6 +144,20 @@ PTY_DEVI void tbase_seq(int t, int& bx, int& by, std::integer_sequence<int, J...
 template <int M, int PASS>
 PTY_DEVI void tbase(int t, int& bx, int& by) {
   tbase_seq<M, PASS>(t, bx, by, std::make_integer_sequence<int, desc<M, PASS>().nt>{});
+}
+// position contributed by the cluster rank in a pass (compile-time bit map)
+template <int M, int PASS>
+PTY_DEVI void rbase(int r, int& bx, int& by) {
+  constexpr PassDesc d = desc<M, PASS>();
+  if constexpr (d.nr > 0) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int pb = j == 0 ? d.rbit[0] : d.rbit[1];
+      const int bit = (r >> j) & 1;
+      if (pb < Plan<M>::LOGM) bx |= bit << pb;
+      else by |= bit << (pb - Plan<M>::LOGM);
+    }
+  }
 }
 
 // unrolled loop whose index is a compile-time constant

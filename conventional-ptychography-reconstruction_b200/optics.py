@@ -28,7 +28,7 @@ from . import _lib
 
 LOSS_CODES = {"smooth_L1_loss": 0, "FD_loss": 1, "Poisson_likelihood_loss": 2}
 _INTENSITY_GRAD = 3
-SUPPORTED_PROBE_SIZES = (64, 128)
+SUPPORTED_PROBE_SIZES = (64, 128, 256)
 
 
 # --------------------------------------------------------------------------

@@ -80,7 +80,8 @@ int ptycho_version(void);
  * batched: for b < B, with f = batch[b],
  *   I_out[b] = | fftshift( fft2( P * O[tlY_f : tlY_f+M, tlX_f : tlX_f+N] ) ) |^2
  * O [H][W] complex64, P [M][N] complex64, I_out [B][M][N] float32.
- * Supported: M == N in {64, 128}.  Needs no scratch memory.
+ * Supported: M == N in {64, 128, 256} (256: one 4-CTA thread-block cluster
+ * per pattern).  Needs no scratch memory.
  * ---------------------------------------------------------------------- */
 int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M, int N,
                              const int32_t* tl, int F, const int32_t* batch, int B,
@@ -101,6 +102,8 @@ int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M
  * added to instead of overwritten.  workspace: device scratch of at least
  * ptycho_fwd_adj_workspace_size() bytes, 256-byte aligned.  Imeas must be
  * 16-byte aligned (each pattern's measurement is fetched by a bulk copy).
+ * M == N in {64, 128, 256}; PTYCHO_LOSS_FD at M = 256 returns
+ * PTYCHO_ERR_UNSUPPORTED_SIZE.
  * ---------------------------------------------------------------------- */
 size_t ptycho_fwd_adj_workspace_size(int H, int W, int M, int N, int B);
 
