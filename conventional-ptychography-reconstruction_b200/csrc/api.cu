@@ -112,7 +112,6 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   int st = check_common(O, H, W, P, M, N, tl, F, batch, B);
   if (st) return st;
   if (loss_type < 0 || loss_type > 3) return PTYCHO_ERR_INVALID_ARG;
-  if (M == 256 && loss_type == PTYCHO_LOSS_FD) return PTYCHO_ERR_UNSUPPORTED_SIZE;
   if (B > 0 && !Imeas) return PTYCHO_ERR_INVALID_ARG;
   if (!pty_aligned(Imeas, 16)) return PTYCHO_ERR_MISALIGNED;
   if ((dO && !pty_aligned(dO, 8)) || (dP && !pty_aligned(dP, 8))) return PTYCHO_ERR_MISALIGNED;

@@ -351,8 +351,7 @@ int launch_fused_m(int mode, int loss, const FusedArgs& a, cudaStream_t s) {
   }
 }
 
-// defined in fused_m64.cu / fused_m128.cu / fused256.cu (4-CTA cluster per
-// pattern; the FD loss is not available at 256 and returns UNSUPPORTED_SIZE)
+// defined in fused_m64.cu / fused_m128.cu / fused256.cu (4-CTA cluster per pattern)
 int launch_fused_64(int mode, int loss, const FusedArgs& a, cudaStream_t s);
 int launch_fused_128(int mode, int loss, const FusedArgs& a, cudaStream_t s);
 int launch_fused_256(int mode, int loss, const FusedArgs& a, cudaStream_t s);

@@ -13,6 +13,7 @@
 //   loss against the measurement rows of this CTA's frequency residue class
 //   (64 bulk copies of 1 KB, mbarrier-tracked, prefetched one pattern ahead);
 //   FP64 per-pattern loss summed over the cluster in rank order via DSMEM
+//   (the FD loss reads its neighbouring frequency rows from the other CTAs)
 //   adjoint: the four passes backwards, the DSMEM exchange reversed, then
 //          E'_b = (-1)^(x+y) dL/dpsi_b written once (same layout as M <= 128).
 // Shared-memory planes are 64 x 256 floats per CTA with no padding: the
@@ -156,6 +157,69 @@ PTY_DEVI void fbase4_seq(int t, int& fx, int& fy, std::integer_sequence<int, J..
   fy = (0 | ... | (((t >> J) & 1) * freq_y<M>(tw_y<M, 4, J>())));
 }
 
+PTY_DEVI float ld_cluster(uint32_t addr) {
+  float v;
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+// FD loss (5-point circular stencil of dW = sqrt(Imeas + eps) - sqrt(I + eps)
+// over the natural frequency grid).  CTA c holds the frequency rows
+// fy = c + 4 j as rows j of its planes, so the rows fy +- 1 are read from the
+// CTAs c +- 1 through distributed shared memory, between cluster barriers.
+// part[e] <- the pixel's loss term; v[e] <- 2 dL/dI v[e].
+PTY_DEVI void fd_terms(float2 (&v)[E], float (&part)[E], int c, int fx0, int fy0, const float* sm, float* re,
+                       float* im, cg::cluster_group& cl) {
+  constexpr float inv_mn = 1.0f / float(M * M);
+  const int j0 = fy0 >> 2;
+  const int c_up = (c + 1) & 3, c_dn = (c + 3) & 3;  // holders of rows fy + 1 and fy - 1
+  const uint32_t im_up = mapa(smem_u32(im), uint32_t(((c_up >> 1) & 1) | ((c_up & 1) << 1)));
+  const uint32_t im_dn = mapa(smem_u32(im), uint32_t(((c_dn >> 1) & 1) | ((c_dn & 1) << 1)));
+  const int dj_up = c == 3 ? 1 : 0, dj_dn = c == 0 ? -1 : 0;
+  float q[E];
+  __syncthreads();  // earlier readers of the planes are done
+  static_for<E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    constexpr int fxe = freq_x<M>(eoff_x<M, 4>(e)), fye = freq_y<M>(eoff_y<M, 4>(e));
+    const int o = (j0 + (fye >> 2)) * M + (fx0 | fxe);
+    const float I = fmaf(v[e].x, v[e].x, v[e].y * v[e].y);
+    im[o] = sqrtf(sm[o] + kEps) - sqrtf(I + kEps);  // dW
+  });
+  cl.sync();  // dW of every row is visible cluster-wide
+  static_for<E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    constexpr int fxe = freq_x<M>(eoff_x<M, 4>(e)), fye = freq_y<M>(eoff_y<M, 4>(e));
+    const int j = j0 + (fye >> 2), fx = fx0 | fxe;
+    const float dw = im[j * M + fx];
+    const float rx = im[j * M + ((fx + 1) & (M - 1))] - dw;
+    const float ry = ld_cluster(im_up + 4u * uint32_t(((j + dj_up) & 63) * M + fx)) - dw;
+    const float G = sqrtf(fmaf(rx, rx, fmaf(ry, ry, kEps)));
+    part[e] = G;
+    re[j * M + fx] = rx / G;
+    q[e] = ry / G;
+  });
+  cl.sync();  // all reads of dW are done; rx / G is visible
+  static_for<E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    constexpr int fxe = freq_x<M>(eoff_x<M, 4>(e)), fye = freq_y<M>(eoff_y<M, 4>(e));
+    const int j = j0 + (fye >> 2), fx = fx0 | fxe;
+    im[j * M + fx] = q[e];  // ry / G
+    q[e] = re[j * M + ((fx - 1) & (M - 1))] - re[j * M + fx];
+  });
+  cl.sync();  // ry / G is visible cluster-wide
+  static_for<E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    constexpr int fxe = freq_x<M>(eoff_x<M, 4>(e)), fye = freq_y<M>(eoff_y<M, 4>(e));
+    const int j = j0 + (fye >> 2), fx = fx0 | fxe;
+    const float up = ld_cluster(im_dn + 4u * uint32_t(((j + dj_dn) & 63) * M + fx));
+    const float dl = (q[e] + up - im[j * M + fx]) * inv_mn;
+    const float I = fmaf(v[e].x, v[e].x, v[e].y * v[e].y);
+    const float g = dl * (-0.5f / sqrtf(I + kEps));
+    v[e] = c_scale(v[e], 2.0f * g);
+  });
+  cl.sync();  // remote reads of this CTA's planes are done before they are reused
+}
+
 template <int MODE, int LOSS>
 __global__ void __launch_bounds__(NT, 1) k_fused256(const FusedArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -296,7 +360,9 @@ __global__ void __launch_bounds__(NT, 1) k_fused256(const FusedArgs a) {
       constexpr float inv_mn = 1.0f / float(M * M);
       float part[E];
       const float* Sb = sm + (fy0 >> 2) * M + fx0;
-      static_for<E>([&](auto ec) {
+      if constexpr (LOSS == PTYCHO_LOSS_FD) {
+        fd_terms(v, part, c, fx0, fy0, sm, re, im, cl);
+      } else static_for<E>([&](auto ec) {
         constexpr int e = decltype(ec)::value;
         constexpr int fxe = freq_x<M>(eoff_x<M, 4>(e)), fye = freq_y<M>(eoff_y<M, 4>(e));
         const float meas = Sb[(fye >> 2) * M + fxe];
@@ -390,16 +456,17 @@ static int launch_t(const FusedArgs& a, cudaStream_t s) {
 int launch_fused_256(int mode, int loss, const FusedArgs& a, cudaStream_t s) {
   using namespace f256;
   if (mode == MODE_INTENSITY) return launch_t<MODE_INTENSITY, 0>(a, s);
-  if (loss == PTYCHO_LOSS_FD) return PTYCHO_ERR_UNSUPPORTED_SIZE;
   if (mode == MODE_LOSS) {
     switch (loss) {
       case 0: return launch_t<MODE_LOSS, 0>(a, s);
+      case 1: return launch_t<MODE_LOSS, 1>(a, s);
       case 2: return launch_t<MODE_LOSS, 2>(a, s);
       default: return launch_t<MODE_LOSS, 3>(a, s);
     }
   }
   switch (loss) {
     case 0: return launch_t<MODE_ADJ, 0>(a, s);
+    case 1: return launch_t<MODE_ADJ, 1>(a, s);
     case 2: return launch_t<MODE_ADJ, 2>(a, s);
     default: return launch_t<MODE_ADJ, 3>(a, s);
   }

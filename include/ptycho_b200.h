@@ -102,8 +102,7 @@ int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M
  * added to instead of overwritten.  workspace: device scratch of at least
  * ptycho_fwd_adj_workspace_size() bytes, 256-byte aligned.  Imeas must be
  * 16-byte aligned (each pattern's measurement is fetched by a bulk copy).
- * M == N in {64, 128, 256}; PTYCHO_LOSS_FD at M = 256 returns
- * PTYCHO_ERR_UNSUPPORTED_SIZE.
+ * M == N in {64, 128, 256}.
  * ---------------------------------------------------------------------- */
 size_t ptycho_fwd_adj_workspace_size(int H, int W, int M, int N, int B);
 

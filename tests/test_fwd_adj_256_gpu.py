@@ -4,8 +4,10 @@ pass-2/pass-3 exchange through distributed shared memory) with the FP64 oracle.
 Tolerances as for 64 / 128 (FP32 FFT against FP64):
   forward intensities  max|I - I_ref| / max|I_ref|      <= 1e-5
   per-pattern losses   |l - l_ref| / |l_ref|            <= 2e-5
-  gradients dO, dP     max|g - g_ref| / max|g_ref|      <= 2e-4
-The FD loss is not provided at 256 (status PTYCHO_ERR_UNSUPPORTED_SIZE).
+  gradients dO, dP     max|g - g_ref| / max|g_ref|      <= 2e-4 (smooth_L1, Poisson),
+                                                         <= 1e-3 (FD)
+The FD stencil couples neighbouring frequency rows, which the cluster keeps in
+different CTAs: its parity also checks the cross-CTA reads.
 """
 import numpy as np
 import pytest
@@ -13,7 +15,7 @@ import torch
 
 from conftest import load_pkg
 from oracle import forward_model as fm
-from test_fwd_adj_gpu import _case, _run, rel_max
+from test_fwd_adj_gpu import GRAD_TOL, _case, _run, rel_max
 
 pytestmark = pytest.mark.gpu
 M = 256
@@ -26,7 +28,7 @@ def pkg():
     return load_pkg()
 
 
-@pytest.mark.parametrize("loss_type", ["smooth_L1_loss", "Poisson_likelihood_loss"])
+@pytest.mark.parametrize("loss_type", fm.LOSS_TYPES)
 @pytest.mark.parametrize("H,B", [(300, 3), (420, 70)])
 def test_against_fp64_oracle_256(pkg, H, B, loss_type):
     # B = 70 exceeds the number of co-resident clusters: the persistent loop runs
@@ -35,8 +37,8 @@ def test_against_fp64_oracle_256(pkg, H, B, loss_type):
     r = fm.fwd_adj(O, P, tlY, tlX, Imeas, loss_type)
     assert np.all(np.abs(lp - r["loss"]) <= 2e-5 * np.abs(r["loss"]) + 1e-12), np.abs(lp / r["loss"] - 1).max()
     assert abs(loss - r["loss_total"]) <= 2e-5 * abs(r["loss_total"])
-    assert rel_max(dO, r["dO"]) <= 2e-4, rel_max(dO, r["dO"])
-    assert rel_max(dP, r["dP"]) <= 2e-4, rel_max(dP, r["dP"])
+    assert rel_max(dO, r["dO"]) <= GRAD_TOL[loss_type], rel_max(dO, r["dO"])
+    assert rel_max(dP, r["dP"]) <= GRAD_TOL[loss_type], rel_max(dP, r["dP"])
 
 
 def test_forward_intensity_256(pkg):
@@ -89,10 +91,12 @@ def test_deterministic_and_edges_256(pkg):
     assert pkg.read_status(dev) == 0
 
 
-def test_fd_loss_unsupported_at_256(pkg):
+def test_fd_loss_only_256(pkg):
+    """FD loss without gradients (loss-only kernel, same cross-CTA stencil)."""
     dev = torch.device("cuda")
-    O, P, tlY, tlX, Imeas = _case(M, 300, 2, seed=23)
-    with pytest.raises(pkg.PtychoError):
-        pkg.fwd_adj_raw(torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev),
-                        pkg.make_windows(tlY, tlX, dev), torch.from_numpy(Imeas).to(dev),
-                        pkg.LOSS_CODES["FD_loss"])
+    O, P, tlY, tlX, Imeas = _case(M, 300, 4, seed=23)
+    loss, lp, _, _ = pkg.fwd_adj_raw(torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev),
+                                     pkg.make_windows(tlY, tlX, dev), torch.from_numpy(Imeas).to(dev),
+                                     pkg.LOSS_CODES["FD_loss"], want_grad=False, per_pattern=True)
+    r = fm.fwd_adj(O, P, tlY, tlX, Imeas, "FD_loss")
+    assert np.all(np.abs(lp.cpu().numpy() - r["loss"]) <= 2e-5 * np.abs(r["loss"]))
