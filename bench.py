@@ -8,8 +8,9 @@ Workload (default ``c1``): 1536^2 complex64 object, 128^2 probe, 40 x 40 raster
 peak, batch 256 patterns per GPU, seeded synthetic data (the reference's
 datasets are not distributed).  One step = one minibatch: the fused
 forward/loss/adjoint kernel plus the deterministic dO/dP assembly (and, for
-N > 1, the NCCL all-reduce of dO and dP -- each rank handles its own
-minibatch, so per-GPU work is fixed: weak scaling).  L2 is flushed (a 256 MiB
+N > 1, the NCCL all-reduce of dP and of the scanned canvas rows of dO --
+each rank draws its minibatch from its own band of the raster, so per-GPU
+work is fixed: weak scaling).  L2 is flushed (a 256 MiB
 write) before every timed step; step times are CUDA events on the launching
 stream, summed over K steps, max over ranks.
 
@@ -199,8 +200,11 @@ def run_reference(args):
 
 
 def _config(w, batch, args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     return {"workload": w.name, "canvas": w.canvas, "probe": w.probe, "positions": w.n_scan ** 2,
             "batch_per_gpu": batch, "loss": w.loss_type, "peak_photons": w.peak,
+            "parallelism": f"dp{world}: scan-row bands per rank, all-reduce of dP and scanned dO rows"
+                           if world > 1 else "dp1",
             "l2": "flushed before every timed step (256 MiB write)"}
 
 
@@ -219,10 +223,19 @@ def run_ours(args):
     stack = torch.from_numpy(work["Imeas"]).to(dev)  # [F, M, M], resident
     F = stack.shape[0]
     H, W = O.shape
-    # each rank draws its own minibatches (seeded per rank)
-    g = torch.Generator().manual_seed(1234 + rank)
+    # each rank draws its minibatches from its own band of the raster (seeded
+    # per rank); a band smaller than B wraps into a second permutation
+    frames = pkg.scan_shards.shard_frames(work["tlY"], work["tlX"], world, rank)
+    rng = np.random.default_rng(1234 + rank)
     nb = args.warmup + args.steps
-    batches = [torch.randperm(F, generator=g)[:B].to(torch.int32).to(dev) for _ in range(nb)]
+
+    def draw():
+        reps = -(-B // frames.size)
+        ids = np.concatenate([frames[rng.permutation(frames.size)] for _ in range(reps)])[:B]
+        return torch.from_numpy(ids.astype(np.int32)).to(dev)
+
+    batches = [draw() for _ in range(nb)]
+    exchange = pkg.scan_shards.GradientExchange(work["tlY"], work["tlX"], M)
     plan = pkg.optics.FwdAdjPlan(O, P, tl, stack, w.loss_type, B)
     dO, dP = plan.dO, plan.dP
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -232,10 +245,7 @@ def run_ours(args):
     def step(i):
         plan.batch.copy_(batches[i])
         plan.replay()
-        if world > 1:
-            import torch.distributed as dist
-            dist.all_reduce(torch.view_as_real(dO))
-            dist.all_reduce(torch.view_as_real(dP))
+        exchange.all_reduce(dO, dP)  # N > 1: dO over the scanned rows, dP (NCCL)
         return plan.loss_total
 
     for i in range(args.warmup):

@@ -35,7 +35,7 @@ import numpy as np
 import torch
 import yaml
 
-from . import optics
+from . import optics, scan_shards
 from .adam import FusedAdam
 from .complex_inr import ComplexINRModel2D
 
@@ -154,10 +154,26 @@ def haar_sparsity(img: torch.Tensor) -> torch.Tensor:
 
 
 class Trainer:
-    """The reference training loop on resident data (one object per run)."""
+    """The reference training loop on resident data (one object per run).
+
+    Under an initialised ``torch.distributed`` process group of more than one
+    rank (one process per GPU), each rank trains on its own band of the
+    raster (``scan_shards``), every rank takes the same number of minibatches
+    per epoch, and the parameter gradients are summed over the ranks after
+    each backward pass, so the model replicas stay identical.  That mode runs
+    eagerly (no CUDA graph holds a collective)."""
 
     def __init__(self, model, stack, tl, loss_type, batch_size, lr, lr_decay_step=10000, lr_decay_gamma=0.1,
                  sparsity_weight=0.0, seed=0, use_graph=True):
+        import torch.distributed as dist
+        self.world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+        self.rank = dist.get_rank() if self.world > 1 else 0
+        if self.world > 1:
+            use_graph = False
+            tl_host = tl.cpu().numpy()
+            self.frames = scan_shards.shard_frames(tl_host[:, 0], tl_host[:, 1], self.world, self.rank)
+            self.steps = scan_shards.steps_per_epoch(int(stack.shape[0]), self.world, int(batch_size))
+            self.np_rng = np.random.default_rng(seed + self.rank)
         self.model = model
         self.stack = stack  # [F, M, M] float32, device
         self.tl = tl        # [F, 2] int32, device
@@ -238,11 +254,18 @@ class Trainer:
         if self.sparsity_weight != 0.0:
             loss = loss + self.sparsity_weight * haar_sparsity(obj)
         loss.backward()
+        if self.world > 1:
+            scan_shards.all_reduce_grads([p for p in self.model.parameters() if p.requires_grad])
         self.opt.step()
         self.last_loss = loss.detach()
         return self.last_loss
 
     def epoch(self):
+        if self.world > 1:
+            for b in scan_shards.epoch_minibatches(self.frames, self.batch_size, self.steps, self.np_rng):
+                self.run(torch.from_numpy(b.astype(np.int32)).to(self.stack.device))
+            self.sched.step()
+            return
         perm = torch.randperm(self.F, device=self.stack.device, generator=self.gen).to(torch.int32)
         for s in range(0, self.F, self.batch_size):
             self.run(perm[s:s + self.batch_size])
