@@ -27,6 +27,9 @@ SIGNATURES = {
     "ptycho_fwd_adj_workspace_size": (_c_size, [_c_int, _c_int, _c_int, _c_int, _c_int]),
     "ptycho_fwd_adj": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _c_int,
                                 _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _c_size, _vp, _vp]),
+    "ptycho_fourier_upsample_workspace_size": (_c_size, [_c_int, _c_int, _c_int]),
+    "ptycho_fourier_upsample": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _vp, _c_size, _vp]),
+    "ptycho_fourier_upsample_adjoint": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _vp, _c_size, _vp]),
     "ptycho_hashgrid_entries": (_c_int, [_c_int, _c_int, _c_int, _c_float]),
     "ptycho_hashgrid_forward": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
     "ptycho_hashgrid_contrib": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp, _vp]),

@@ -3,10 +3,11 @@
 Same constructor, attributes (``xy_coords``, ``probe_coords``,
 ``k_object``, ``k_probe``, ``has_*_residual``, ``downsampled_*``) and
 ``forward() -> (object_complex [W, H], probe_complex [Wp, Hp] or None)``.
-The hash encoders are :class:`hashgrid.Encoding` (tiny-cuda-nn's interface)
-and the MLPs :class:`cmlp.ComplexMLP` (fused tensor-core kernels).  The
-Fourier upsampling of the object (models/complex_inr.py:252-271) uses the
-same torch.fft formula as the reference.
+The hash encoders are :class:`hashgrid.Encoding` (tiny-cuda-nn's interface),
+the MLPs :class:`cmlp.ComplexMLP` (fused tensor-core kernels) and the Fourier
+upsampling of the object (models/complex_inr.py:252-271) the shared-memory
+FFT resampling kernels of :mod:`resample` (power-of-two sizes; the torch.fft
+formula otherwise).
 """
 from __future__ import annotations
 
@@ -14,6 +15,7 @@ import torch
 import torch.nn as nn
 import torch.nn.functional as F
 
+from . import resample
 from .cmlp import ComplexMLP
 from .hashgrid import Encoding
 
@@ -91,8 +93,13 @@ class ComplexINRModel2D(nn.Module):
             self.has_probe_residual = False
 
     def fourier_upsample(self, x, scale_factor):
-        """fftshift(fft2) -> zero-pad -> ifftshift -> ifft2, times scale^2 (:252-271)."""
+        """fftshift(fft2) -> zero-pad -> ifftshift -> ifft2, times scale^2 (:252-271).
+
+        Power-of-two sizes run on the resampling kernels (``resample``); other
+        shapes keep the reference's torch.fft formula."""
         B, C, H, W = x.shape
+        if B == 1 and C == 1 and x.is_cuda and resample.supported(H, W, scale_factor):
+            return resample.fourier_upsample(x[0, 0], int(scale_factor))[None, None]
         x_fft = torch.fft.fftshift(torch.fft.fft2(x, dim=(-2, -1)), dim=(-2, -1))
         nH, nW = int(H * scale_factor), int(W * scale_factor)
         ph, pw = (nH - H) // 2, (nW - W) // 2

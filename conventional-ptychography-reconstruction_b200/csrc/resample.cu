@@ -1,0 +1,290 @@
+// resample.cu -- Fourier (band-limited) upsampling of the object and its adjoint.
+//
+// Replaces models/complex_inr.py:252-271 (called at :287):
+//   y = ifft2( ifftshift( zero_pad( fftshift( fft2(x) ) ) ) ) * s^2,
+// x [h][w] -> y [h*s][w*s] complex64, and the gradient of that map (torch's
+// complex convention, the conjugate-transpose operator).  The map is
+// separable: per axis, y = (s / N) F_N^-1 P F_n x, where F is the
+// unnormalised DFT and P places frequency f in [-n/2, n/2) of the length-n
+// spectrum at f mod N of the length-N one (for even n and N this is what the
+// shift / centred pad / inverse shift of the reference does).  Its adjoint is
+// (s / N) F_n^-1 P^T F_N.  Both are "forward FFT of length L1, spectrum remap,
+// inverse FFT of length L2, scale 1 / min(L1, L2)", so one kernel does all
+// four line transforms:
+//   row pass    -- lines are rows (contiguous), written as rows;
+//   column pass -- lines are LINES adjacent columns (32-byte or wider
+//                  segments per row), written the same way.
+// Upsampling: row pass x -> t [h][w s], column pass t -> y.  Adjoint: row pass
+// g -> t [h s][w], column pass t -> x-gradient.
+//
+// Each CTA loads LINES lines into two shared-memory planes (re, im; one float
+// of padding every 32), runs radix-16 (then 8/4/2) Stockham passes -- natural
+// order in and out, each thread holding one or two 16-value slots in
+// registers, in place between barriers -- remaps the spectrum, runs the
+// inverse passes and writes the lines back.  Twiddles come from a per-CTA
+// table exp(-2 pi i k / LMAX) rounded from double-precision sincospi.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "dft_regs.cuh"
+
+namespace pty {
+namespace rs {
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int cmin(int a, int b) { return a < b ? a : b; }
+
+template <int L1, int L2, bool COL>
+struct Cfg {
+  static constexpr int LMAX = cmax(L1, L2);
+  // row pass: 2048 values per CTA (>= 1 line); column pass: >= 4 lines
+  // (32-byte segments) and 4096 values per CTA when lines are short
+  static constexpr int LINES = COL ? cmax(4, 4096 / LMAX) : cmax(1, 2048 / LMAX);
+  static constexpr int N = LINES * LMAX;            // values held by the CTA
+  static constexpr int NT = cmin(512, N / 16);      // threads: one 16-value slot each, or two
+  static constexpr int SPT = N / 16 / NT;           // slots per thread (1 or 2)
+  static constexpr int PLANE = N + N / 32;          // padded plane length (floats)
+  static constexpr size_t SMEM = size_t(2) * PLANE * 4 + size_t(LMAX) * 8;
+  static_assert(SPT == 1 || SPT == 2, "slot count");
+  static_assert(L1 >= 64 && L2 >= 64 && LMAX <= 4096, "supported line lengths");
+};
+
+PTY_DEVI int pad(int i) { return i + (i >> 5); }
+
+// One Stockham pass of radix R over every line of length L: butterfly j of a
+// line reads j + r L/R, applies exp(-+2 pi i (j mod NS) r / (NS R)) and the
+// radix-R DFT, and writes (j / NS) NS R + (j mod NS) + r NS.
+template <int L, int R, int NS, bool INV, int LINES, int NT, int SPT, int LMAX>
+PTY_DEVI void stockham(float* re, float* im, const float2* __restrict__ tw, int t) {
+  constexpr int BPL = L / R;              // butterflies per line
+  constexpr int NB = LINES * BPL;         // butterflies in the CTA
+  constexpr int PER = 16 / R;             // butterflies per 16-value slot
+  constexpr int NSLOT = NB / PER;         // slots in use (<= SPT * NT)
+  constexpr int TWS = LMAX / (NS * R);    // twiddle table stride
+  float2 v[SPT][16];
+  int jj[SPT][PER], base[SPT][PER];
+#pragma unroll
+  for (int q = 0; q < SPT; ++q) {
+    const int s = t + q * NT;
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int b = s + p * NSLOT;  // consecutive lanes -> consecutive j
+      const int line = b / BPL, j = b - line * BPL;
+      jj[q][p] = j;
+      base[q][p] = line * LMAX;
+      if (s < NSLOT) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = pad(base[q][p] + j + r * BPL);
+          v[q][p * R + r] = make_float2(re[i], im[i]);
+        }
+      }
+    }
+  }
+  __syncthreads();  // every value is read before any is overwritten
+#pragma unroll
+  for (int q = 0; q < SPT; ++q) {
+    const int s = t + q * NT;
+    if (s < NSLOT) {
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int j = jj[q][p];
+        const int k = j % NS;
+        if constexpr (NS > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            float2 w = tw[k * r * TWS];
+            if constexpr (INV) w.y = -w.y;
+            v[q][p * R + r] = c_mul(v[q][p * R + r], w);
+          }
+        }
+        dft<R, INV, 1>(&v[q][p * R]);
+        const int o = base[q][p] + (j / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = pad(o + r * NS);
+          re[i] = v[q][p * R + r].x;
+          im[i] = v[q][p * R + r].y;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// all passes of a length-L transform: radix 16 while 16 divides the rest, then 8/4/2
+template <int L, bool INV, int LINES, int NT, int SPT, int LMAX, int NS = 1>
+PTY_DEVI void fft_lines(float* re, float* im, const float2* tw, int t) {
+  if constexpr (NS < L) {
+    constexpr int REST = L / NS;
+    constexpr int R = REST >= 16 ? 16 : REST;
+    stockham<L, R, NS, INV, LINES, NT, SPT, LMAX>(re, im, tw, t);
+    fft_lines<L, INV, LINES, NT, SPT, LMAX, NS * R>(re, im, tw, t);
+  }
+}
+
+template <int L1, int L2, bool COL>
+__global__ void __launch_bounds__(Cfg<L1, L2, COL>::NT) k_resample(const float2* __restrict__ in,
+                                                                   float2* __restrict__ out, int nlines,
+                                                                   long long ld_in, long long ld_out,
+                                                                   float scale) {
+  using C = Cfg<L1, L2, COL>;
+  constexpr int LINES = C::LINES, NT = C::NT, LMAX = C::LMAX;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* re = reinterpret_cast<float*>(smem);
+  float* im = re + C::PLANE;
+  float2* tw = reinterpret_cast<float2*>(im + C::PLANE);
+  const int t = threadIdx.x;
+  const int l0 = blockIdx.x * LINES;
+  for (int k = t; k < LMAX; k += NT) {
+    double s, c;
+    sincospi(-2.0 * double(k) / double(LMAX), &s, &c);
+    tw[k] = make_float2(float(c), float(s));
+  }
+  // load LINES lines of length L1 (lines past the end read as zero)
+  for (int idx = t; idx < LINES * L1; idx += NT) {
+    int l, k;
+    if constexpr (COL) {
+      l = idx % LINES;
+      k = idx / LINES;
+    } else {
+      l = idx / L1;
+      k = idx - l * L1;
+    }
+    float2 x = make_float2(0.f, 0.f);
+    if (l0 + l < nlines)
+      x = COL ? __ldg(in + k * ld_in + (l0 + l)) : __ldg(in + (l0 + l) * ld_in + k);
+    const int i = pad(l * LMAX + k);
+    re[i] = x.x;
+    im[i] = x.y;
+  }
+  __syncthreads();
+  fft_lines<L1, false, LINES, NT, C::SPT, LMAX>(re, im, tw, t);
+  // spectrum remap: frequency f in [-n/2, n/2), n = min(L1, L2), from f mod L1 to f mod L2
+  if constexpr (L2 > L1) {
+    for (int idx = t; idx < LINES * (L1 / 2); idx += NT) {  // negative frequencies move up
+      const int l = idx / (L1 / 2), k = L1 / 2 + (idx - l * (L1 / 2));
+      const int a = pad(l * LMAX + k), b = pad(l * LMAX + k + (L2 - L1));
+      re[b] = re[a];
+      im[b] = im[a];
+    }
+    __syncthreads();
+    for (int idx = t; idx < LINES * (L2 - L1); idx += NT) {  // the new band is empty
+      const int l = idx / (L2 - L1), k = L1 / 2 + (idx - l * (L2 - L1));
+      const int a = pad(l * LMAX + k);
+      re[a] = 0.f;
+      im[a] = 0.f;
+    }
+    __syncthreads();
+  } else if constexpr (L2 < L1) {
+    for (int idx = t; idx < LINES * (L2 / 2); idx += NT) {  // negative frequencies move down
+      const int l = idx / (L2 / 2), k = L2 / 2 + (idx - l * (L2 / 2));
+      const int a = pad(l * LMAX + k + (L1 - L2)), b = pad(l * LMAX + k);
+      re[b] = re[a];
+      im[b] = im[a];
+    }
+    __syncthreads();
+  }
+  fft_lines<L2, true, LINES, NT, C::SPT, LMAX>(re, im, tw, t);
+  for (int idx = t; idx < LINES * L2; idx += NT) {
+    int l, k;
+    if constexpr (COL) {
+      l = idx % LINES;
+      k = idx / LINES;
+    } else {
+      l = idx / L2;
+      k = idx - l * L2;
+    }
+    if (l0 + l < nlines) {
+      const int i = pad(l * LMAX + k);
+      const float2 y = make_float2(re[i] * scale, im[i] * scale);
+      if constexpr (COL)
+        out[k * ld_out + (l0 + l)] = y;
+      else
+        out[(l0 + l) * ld_out + k] = y;
+    }
+  }
+}
+
+template <int L1, int L2, bool COL>
+int launch(const float2* in, float2* out, int nlines, long long ld_in, long long ld_out, cudaStream_t s) {
+  using C = Cfg<L1, L2, COL>;
+  auto kern = k_resample<L1, L2, COL>;
+  if (C::SMEM > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::SMEM)) != cudaSuccess)
+    return PTYCHO_ERR_LAUNCH;
+  const int grid = (nlines + C::LINES - 1) / C::LINES;
+  kern<<<grid, C::NT, C::SMEM, s>>>(in, out, nlines, ld_in, ld_out, 1.0f / float(L1 < L2 ? L1 : L2));
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+// dispatch over line lengths 2^6 .. 2^12 with L2 / L1 in {1/4, 1/2, 1, 2, 4}
+template <bool COL>
+int dispatch(int l1, int l2, const float2* in, float2* out, int nlines, long long ld_in, long long ld_out,
+             cudaStream_t s) {
+#define PTY_RS(A, B) \
+  if (l1 == A && l2 == B) return launch<A, B, COL>(in, out, nlines, ld_in, ld_out, s);
+#define PTY_RS_ROW(A) PTY_RS(A, A) PTY_RS(A, 2 * A) PTY_RS(2 * A, A) PTY_RS(A, 4 * A) PTY_RS(4 * A, A)
+  PTY_RS_ROW(64)
+  PTY_RS_ROW(128)
+  PTY_RS_ROW(256)
+  PTY_RS_ROW(512)
+  PTY_RS_ROW(1024)
+  PTY_RS(2048, 2048) PTY_RS(2048, 4096) PTY_RS(4096, 2048)
+  PTY_RS(4096, 4096)
+#undef PTY_RS_ROW
+#undef PTY_RS
+  return PTYCHO_ERR_UNSUPPORTED_SIZE;
+}
+
+bool supported(int n, int N) {
+  auto pow2 = [](int v) { return v >= 64 && v <= 4096 && (v & (v - 1)) == 0; };
+  if (!pow2(n) || !pow2(N)) return false;
+  const int r = n > N ? n / N : N / n;
+  return r == 1 || r == 2 || r == 4;
+}
+
+}  // namespace rs
+}  // namespace pty
+
+using namespace pty;
+
+extern "C" {
+
+size_t ptycho_fourier_upsample_workspace_size(int h, int w, int s) {
+  if (h <= 0 || w <= 0 || s <= 0) return 0;
+  return size_t(h) * size_t(w) * size_t(s) * sizeof(float2);
+}
+
+int ptycho_fourier_upsample(const float* x, int h, int w, int s, float* y, void* workspace,
+                            size_t workspace_bytes, ptycho_stream_t stream) {
+  if (!x || !y || h <= 0 || w <= 0 || s <= 0) return PTYCHO_ERR_INVALID_ARG;
+  if (!rs::supported(h, h * s) || !rs::supported(w, w * s)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  if (!workspace || workspace_bytes < ptycho_fourier_upsample_workspace_size(h, w, s))
+    return PTYCHO_ERR_WORKSPACE;
+  if (!pty_aligned(x, 8) || !pty_aligned(y, 8) || !pty_aligned(workspace, 8)) return PTYCHO_ERR_MISALIGNED;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int W = w * s, H = h * s;
+  float2* tmp = static_cast<float2*>(workspace);
+  int rc = rs::dispatch<false>(w, W, reinterpret_cast<const float2*>(x), tmp, h, w, W, st);  // rows
+  if (rc) return rc;
+  return rs::dispatch<true>(h, H, tmp, reinterpret_cast<float2*>(y), W, W, W, st);           // columns
+}
+
+int ptycho_fourier_upsample_adjoint(const float* gy, int h, int w, int s, float* gx, void* workspace,
+                                    size_t workspace_bytes, ptycho_stream_t stream) {
+  if (!gy || !gx || h <= 0 || w <= 0 || s <= 0) return PTYCHO_ERR_INVALID_ARG;
+  if (!rs::supported(h, h * s) || !rs::supported(w, w * s)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  if (!workspace || workspace_bytes < ptycho_fourier_upsample_workspace_size(h, w, s))
+    return PTYCHO_ERR_WORKSPACE;
+  if (!pty_aligned(gy, 8) || !pty_aligned(gx, 8) || !pty_aligned(workspace, 8)) return PTYCHO_ERR_MISALIGNED;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int W = w * s, H = h * s;
+  float2* tmp = static_cast<float2*>(workspace);  // [H][w]
+  int rc = rs::dispatch<false>(W, w, reinterpret_cast<const float2*>(gy), tmp, H, W, w, st);  // rows
+  if (rc) return rc;
+  return rs::dispatch<true>(H, h, tmp, reinterpret_cast<float2*>(gx), w, w, w, st);           // columns
+}
+
+}  // extern "C"

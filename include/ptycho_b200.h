@@ -202,6 +202,27 @@ int ptycho_adam_step_dev(float* const* params, const float* const* grads, float*
                          ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Fourier upsampling of the INR object.  Replaces fourier_upsample of
+ * models/complex_inr.py:252-271 (called at :287):
+ *   y = ifft2(ifftshift(pad(fftshift(fft2(x))))) * s^2,
+ * x [h][w] complex64 -> y [h*s][w*s] complex64, the pad centred at
+ * ((h*s - h)/2, (w*s - w)/2).  The adjoint maps an upstream gradient gy
+ * [h*s][w*s] to gx [h][w] (torch's complex convention; the operator's
+ * conjugate transpose).  h, w, h*s and w*s must be powers of two in
+ * [64, 4096] with s in {1, 2, 4}; otherwise PTYCHO_ERR_UNSUPPORTED_SIZE.
+ * workspace: device scratch of ptycho_fourier_upsample_workspace_size()
+ * bytes (the intermediate after the row pass), 8-byte aligned.
+ * ---------------------------------------------------------------------- */
+size_t ptycho_fourier_upsample_workspace_size(int h, int w, int s);
+
+int ptycho_fourier_upsample(const float* x, int h, int w, int s, float* y, void* workspace,
+                            size_t workspace_bytes, ptycho_stream_t stream);
+
+int ptycho_fourier_upsample_adjoint(const float* gy, int h, int w, int s, float* gx,
+                                    void* workspace, size_t workspace_bytes,
+                                    ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
  * must not trigger an allocation's device synchronisation).  No counterpart

@@ -65,6 +65,20 @@ def test_validation_before_device_work():
                                       fake, None, None) == 3
 
 
+def test_fourier_upsample_validation_before_device_work():
+    L = load_pkg().lib()
+    st = {"INVALID_ARG": 1, "UNSUPPORTED_SIZE": 2, "MISALIGNED": 3, "WORKSPACE": 4}  # include/ptycho_b200.h
+    fake = ctypes.c_void_p(4096)  # never dereferenced: validation fails first
+    n = L.ptycho_fourier_upsample_workspace_size(512, 512, 2)
+    assert n == 512 * 512 * 2 * 8 and L.ptycho_fourier_upsample_workspace_size(0, 8, 2) == 0
+    for fn in (L.ptycho_fourier_upsample, L.ptycho_fourier_upsample_adjoint):
+        assert fn(fake, 96, 96, 2, fake, fake, n, None) == st["UNSUPPORTED_SIZE"]
+        assert fn(fake, 64, 64, 8, fake, fake, n, None) == st["UNSUPPORTED_SIZE"]
+        assert fn(None, 64, 64, 2, fake, fake, n, None) == st["INVALID_ARG"]
+        assert fn(fake, 512, 512, 2, fake, fake, n - 8, None) == st["WORKSPACE"]
+        assert fn(ctypes.c_void_p(4100), 512, 512, 2, fake, fake, n, None) == st["MISALIGNED"]
+
+
 def test_workspace_size_monotone():
     L = load_pkg().lib()
     a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)
