@@ -30,6 +30,11 @@ SIGNATURES = {
     "ptycho_fourier_upsample_workspace_size": (_c_size, [_c_int, _c_int, _c_int]),
     "ptycho_fourier_upsample": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _vp, _c_size, _vp]),
     "ptycho_fourier_upsample_adjoint": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _vp, _c_size, _vp]),
+    "ptycho_probe_center_normalize": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
+    "ptycho_probe_center_normalize_backward": (_c_int, [_vp, _vp, _vp, _c_int, _c_int, _vp, _vp]),
+    "ptycho_haar_sparsity_workspace_size": (_c_size, [_c_int, _c_int]),
+    "ptycho_haar_sparsity": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _c_size, _vp]),
+    "ptycho_haar_sparsity_backward": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     "ptycho_hashgrid_entries": (_c_int, [_c_int, _c_int, _c_int, _c_float]),
     "ptycho_hashgrid_forward": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
     "ptycho_hashgrid_contrib": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp, _vp]),

@@ -35,7 +35,7 @@ import numpy as np
 import torch
 import yaml
 
-from . import optics, scan_shards
+from . import optics, probe_prep, scan_shards
 from .adam import FusedAdam
 from .complex_inr import ComplexINRModel2D
 
@@ -124,33 +124,14 @@ class PixelGrid(torch.nn.Module):
 
 def center_and_normalize_probe(P: torch.Tensor) -> torch.Tensor:
     """Centre-of-mass roll (Recovery.py:262-278) and energy scaling to
-    sum|P|^2 = M*N (:282-285), on the device: the roll amount is a device
-    tensor applied by index arithmetic, the energy test is a select."""
-    M, N = P.shape
-    dev = P.device
-    with torch.no_grad():
-        a = P.detach().abs() ** 2
-        tot = a.sum()
-        safe = torch.where(tot == 0, torch.ones_like(tot), tot)
-        cy = torch.trunc(M / 2 - M * a.sum(1).cumsum(0).mean() / safe + 1)
-        cx = torch.trunc(N / 2 - N * a.sum(0).cumsum(0).mean() / safe + 1)
-        cy = torch.where(tot == 0, torch.zeros_like(cy), cy).long()
-        cx = torch.where(tot == 0, torch.zeros_like(cx), cx).long()
-        iy = (torch.arange(M, device=dev) + cy) % M
-        ix = (torch.arange(N, device=dev) + cx) % N
-    P = P[iy][:, ix]  # == torch.roll(P, (-cp0, -cp1), (0, 1))
-    e = (P.abs() ** 2).sum()
-    scale = torch.where(e > 0, torch.sqrt(float(M * N) / torch.where(e > 0, e, torch.ones_like(e))),
-                        torch.ones_like(e))
-    return P * scale
+    sum|P|^2 = M*N (:282-285): one device kernel each way, no host syncs."""
+    return probe_prep.center_and_normalize_probe(P)
 
 
 def haar_sparsity(img: torch.Tensor) -> torch.Tensor:
-    """L1 of the LH/HL/HH Haar subbands of Re and Im (utils/loss.py:60-83)."""
-    if torch.is_complex(img):
-        return haar_sparsity(img.real) + haar_sparsity(img.imag)
-    a, b, c, d = img[0::2, 0::2], img[0::2, 1::2], img[1::2, 0::2], img[1::2, 1::2]
-    return (a - b + c - d).abs().sum() + (a + b - c - d).abs().sum() + (a - b - c + d).abs().sum()
+    """L1 of the LH/HL/HH Haar subbands of Re and Im (utils/loss.py:60-83),
+    on the device kernels (FP64 reduction, no host syncs)."""
+    return probe_prep.haar_sparsity(img)
 
 
 class Trainer:

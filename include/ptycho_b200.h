@@ -223,6 +223,42 @@ int ptycho_fourier_upsample_adjoint(const float* gy, int h, int w, int s, float*
                                     ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Probe preparation.  Replaces the per-minibatch probe centring and
+ * normalisation of Recovery.py:262-285 (utils center_probe's centre-of-mass
+ * roll, then scaling to sum |P|^2 = M*N), without host synchronisation:
+ *   cp = trunc([M, N]/2 - [M, N] * mean(cumsum(marginal |P|^2)) / tot + 1)
+ *   P_out = sqrt(M N / e) * roll(P, -cp),  e = sum |P|^2   (no change if e == 0)
+ * P, P_out [M][N] complex64 (distinct buffers), M, N <= 1024.  state [4]
+ * doubles receives {cp_y, cp_x, scale, e} for the backward.  Sums are FP64
+ * in a fixed order.  The backward maps the gradient of P_out to that of P
+ * (torch's complex convention), including the term through e.
+ * ---------------------------------------------------------------------- */
+int ptycho_probe_center_normalize(const float* P, int M, int N, float* P_out, double* state,
+                                  ptycho_stream_t stream);
+
+int ptycho_probe_center_normalize_backward(const float* P_out, const double* state,
+                                           const float* grad_out, int M, int N, float* grad_in,
+                                           ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
+ * Haar-wavelet sparsity.  Replaces haar_wavelet_sparsity_loss
+ * (utils/loss.py:60-83; used at Recovery.py:309-313): the L1 norm of the
+ * three detail subbands of the 2x2 Haar transform of img [H][W] complex64
+ * (real and imaginary parts separately), as one FP64 value *loss_out
+ * (device), summed in a fixed order.  H and W must be even.  workspace:
+ * ptycho_haar_sparsity_workspace_size() bytes.  The backward writes
+ * grad_img = (*grad_loss) * d loss / d img (torch's complex convention,
+ * sign(0) = 0), grad_loss being a device double.
+ * ---------------------------------------------------------------------- */
+size_t ptycho_haar_sparsity_workspace_size(int H, int W);
+
+int ptycho_haar_sparsity(const float* img, int H, int W, double* loss_out, void* workspace,
+                         size_t workspace_bytes, ptycho_stream_t stream);
+
+int ptycho_haar_sparsity_backward(const float* img, int H, int W, const double* grad_loss,
+                                  float* grad_img, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
  * must not trigger an allocation's device synchronisation).  No counterpart

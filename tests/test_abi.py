@@ -79,6 +79,20 @@ def test_fourier_upsample_validation_before_device_work():
         assert fn(ctypes.c_void_p(4100), 512, 512, 2, fake, fake, n, None) == st["MISALIGNED"]
 
 
+def test_probe_prep_and_haar_validation_before_device_work():
+    L = load_pkg().lib()
+    fake = ctypes.c_void_p(4096)  # never dereferenced: validation fails first
+    other = ctypes.c_void_p(8192)
+    assert L.ptycho_probe_center_normalize(None, 64, 64, fake, other, None) == 1
+    assert L.ptycho_probe_center_normalize(fake, 64, 64, fake, other, None) == 1  # in place refused
+    assert L.ptycho_probe_center_normalize(fake, 2048, 64, other, other, None) == 2
+    assert L.ptycho_probe_center_normalize_backward(fake, fake, fake, 64, 64, fake, None) == 1
+    assert L.ptycho_haar_sparsity_workspace_size(1536, 1536) == 576 * 8
+    assert L.ptycho_haar_sparsity(fake, 63, 64, fake, fake, 4096, None) == 2
+    assert L.ptycho_haar_sparsity(fake, 64, 64, fake, fake, 0, None) == 4
+    assert L.ptycho_haar_sparsity_backward(fake, 64, 65, fake, fake, None) == 2
+
+
 def test_workspace_size_monotone():
     L = load_pkg().lib()
     a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)
