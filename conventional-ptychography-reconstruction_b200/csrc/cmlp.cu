@@ -10,8 +10,11 @@
 //   y  = Wo h3 + bo (complex 1x32).
 // A complex layer acts on [Re h; Im h] as the real 64x64 block [[A,-B],[B,A]]
 // (W = A + iB).  Operands are BF16 in shared memory, accumulators FP32 in
-// tensor memory; one CTA (128 threads, thread t = row t) handles tiles of 128
-// coordinates and loops over tiles (persistent).
+// tensor memory; one CTA handles tiles of 128 coordinates and loops over
+// tiles (persistent).  256 threads: warp w reads TMEM lane quarter w & 3 (tile
+// rows 32 (w & 3) .. +31) and does the elementwise work of half w >> 2 of each
+// layer's complex units, so the sin / cos / exp chains between two MMAs are
+// split over 8 warps.
 //
 // Backward (training): the kernel recomputes the forward of its tile, then
 //   G_h3 = Wo_r^T G_y,  G_z = conj(i w h) G_h (complex layers),
@@ -35,7 +38,7 @@
 namespace pty {
 namespace cm {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;
 constexpr int GRP = 2048;  // one group of 8 bf16 features x 128 rows
 
 // ---- shared-memory map (bytes) --------------------------------------------
@@ -47,16 +50,16 @@ constexpr int kWBytes = S_WO + 2048;  // 20480
 constexpr int S_PAR = kWBytes;      // fp32 biases and omegas
 constexpr int S_BAR = S_PAR + 1024;
 constexpr int S_TMEM = S_BAR + 16;
-constexpr int S_RED = S_TMEM + 16;
-constexpr int S_X = S_RED + 64;     // 6 groups: x (4), ones, zeros
+constexpr int S_RED = S_TMEM + 16;  // 24 floats: omega-gradient partials of 8 warps
+constexpr int S_X = S_RED + 128;    // 6 groups: x (4), ones, zeros
 constexpr int S_H = S_X + 6 * GRP;  // 18 groups: h2 (8), h1 (8), ones, zeros
 constexpr int S_H3 = S_H + 18 * GRP;  // 10 groups: h3 (8), ones, zeros
 constexpr int S_GY = S_H3 + 10 * GRP;  // 2 groups: (G_yr, G_yi, 0, ...), zeros
 constexpr int S_GZ1 = S_GY + 2 * GRP;  // 4 groups: G_z1
 constexpr int S_GZ = S_GZ1 + 4 * GRP;  // 16 groups: G_z3 (8), G_z2 (8)
 constexpr int S_ACT_END = S_GZ + 16 * GRP;
-constexpr int kSmemBwd = S_ACT_END;  // 136288 bytes: one CTA per SM
-constexpr int kSmemFwd = S_GY;       // 91200 bytes: the forward needs x, h, h3 only -> two CTAs per SM
+constexpr int kSmemBwd = S_ACT_END;  // 136352 bytes: one CTA per SM
+constexpr int kSmemFwd = S_GY;       // 91264 bytes: the forward needs x, h, h3 only -> two CTAs per SM
 
 // every MMA footprint used below stays inside [0, S_ACT_END)
 static_assert(S_GY + 16 * GRP <= S_ACT_END, "output-grad A footprint");
@@ -144,9 +147,12 @@ struct Args {
 };
 
 template <bool BWD>
-__global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
+__global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int t = threadIdx.x, w = t >> 5;
+  const int quarter = w & 3;                // TMEM lane quarter of this warp
+  const int hh = w >> 2;                    // half of each layer's units handled here
+  const int row = 32 * quarter + (t & 31);  // tile row (TMEM lane) of this thread
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S_BAR);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + S_TMEM);
   float* par = reinterpret_cast<float*>(sm + S_PAR);
@@ -163,11 +169,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
   for (int i = t; i < kParFloats; i += kThreads)
     par[i] = __ldg(reinterpret_cast<const float*>(a.packed + kWBytes) + i);
   __syncthreads();
-  {
+  if (hh == 0) {
     const __nv_bfloat16 one = __float2bfloat16(1.0f);
-    *reinterpret_cast<__nv_bfloat16*>(sm + S_X + cm_off(t, 32)) = one;
-    *reinterpret_cast<__nv_bfloat16*>(sm + S_H + cm_off(t, 128)) = one;
-    *reinterpret_cast<__nv_bfloat16*>(sm + S_H3 + cm_off(t, 64)) = one;
+    *reinterpret_cast<__nv_bfloat16*>(sm + S_X + cm_off(row, 32)) = one;
+    *reinterpret_cast<__nv_bfloat16*>(sm + S_H + cm_off(row, 128)) = one;
+    *reinterpret_cast<__nv_bfloat16*>(sm + S_H3 + cm_off(row, 64)) = one;
   }
   if (t == 0) {
     mbar_init(bar, 1);
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
   __syncthreads();
   tc::fence_after();
   const uint32_t tm = *tslot;
-  const uint32_t lo = uint32_t(w * 32) << 16;  // this warp's TMEM lane quarter
+  const uint32_t lo = uint32_t(quarter * 32) << 16;  // this warp's TMEM lane quarter
   const float w1 = par[P_W1], w2 = par[P_W2], w3 = par[P_W3];
   uint32_t phase = 0;
   bool abort = false;
@@ -206,47 +212,49 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
   bool first = true;
   const int ntiles = (a.N + 127) / 128;
   for (int tile = blockIdx.x; tile < ntiles && !abort; tile += gridDim.x) {
-    const int c = tile * 128 + t;
+    const int c = tile * 128 + row;
     const bool valid = c < a.N;
-    // -- inputs ----------------------------------------------------------------
+    // -- inputs: this half's 16 of the row's 32 features ------------------------
     {
-      float xv[32];
-      const float4* xp = reinterpret_cast<const float4*>(a.x + size_t(valid ? c : 0) * 32);
+      float xv[16];
+      const float4* xp = reinterpret_cast<const float4*>(a.x + size_t(valid ? c : 0) * 32 + 16 * hh);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < 4; ++q) {
         const float4 v = valid ? __ldg(xp + q) : make_float4(0.f, 0.f, 0.f, 0.f);
         xv[4 * q] = v.x;
         xv[4 * q + 1] = v.y;
         xv[4 * q + 2] = v.z;
         xv[4 * q + 3] = v.w;
       }
-#pragma unroll
-      for (int g = 0; g < 4; ++g) st8(sm + S_X, t, 8 * g, xv + 8 * g);
+      st8(sm + S_X, row, 16 * hh, xv);
+      st8(sm + S_X, row, 16 * hh + 8, xv + 8);
       if constexpr (BWD) {
-        const float2 g = valid ? __ldg(a.gy + c) : make_float2(0.f, 0.f);
-        const float v8[8] = {g.x, g.y, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        st8(sm + S_GY, t, 0, v8);
+        if (hh == 0) {
+          const float2 g = valid ? __ldg(a.gy + c) : make_float2(0.f, 0.f);
+          const float v8[8] = {g.x, g.y, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+          st8(sm + S_GY, row, 0, v8);
+        }
       }
     }
     // -- layer 1 ---------------------------------------------------------------
     step([&] { gemm_act_w(tm + T_D1, sbase + S_X, sbase + S_W1, 32, 32, 32, false); });
     if (abort) break;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    {
+      const int h = hh;
       float d[16], hr[16], hi[16];
       tc::ld16(tm + lo + T_D1 + 16 * h, d);
 #pragma unroll
       for (int k = 0; k < 16; ++k) sincos_rr(w1 * (d[k] + par[P_B1 + 16 * h + k]), &hi[k], &hr[k]);
-      st8(sm + S_H, t, 64 + 16 * h, hr);
-      st8(sm + S_H, t, 72 + 16 * h, hr + 8);
-      st8(sm + S_H, t, 96 + 16 * h, hi);
-      st8(sm + S_H, t, 104 + 16 * h, hi + 8);
+      st8(sm + S_H, row, 64 + 16 * h, hr);
+      st8(sm + S_H, row, 72 + 16 * h, hr + 8);
+      st8(sm + S_H, row, 96 + 16 * h, hi);
+      st8(sm + S_H, row, 104 + 16 * h, hi + 8);
     }
     // -- complex layers 2 and 3 ------------------------------------------------
     step([&] { gemm_act_w(tm + T_D2, sbase + S_H + 8 * GRP, sbase + S_W2, 64, 64, 64, false); });
     if (abort) break;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    {
+      const int h = hh;
       float zr[16], zi[16], hr[16], hi[16];
       tc::ld16(tm + lo + T_D2 + 16 * h, zr);
       tc::ld16(tm + lo + T_D2 + 32 + 16 * h, zi);
@@ -259,15 +267,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
         hr[k] = amp * co;
         hi[k] = amp * s;
       }
-      st8(sm + S_H, t, 16 * h, hr);
-      st8(sm + S_H, t, 8 + 16 * h, hr + 8);
-      st8(sm + S_H, t, 32 + 16 * h, hi);
-      st8(sm + S_H, t, 40 + 16 * h, hi + 8);
+      st8(sm + S_H, row, 16 * h, hr);
+      st8(sm + S_H, row, 8 + 16 * h, hr + 8);
+      st8(sm + S_H, row, 32 + 16 * h, hi);
+      st8(sm + S_H, row, 40 + 16 * h, hi + 8);
     }
     step([&] { gemm_act_w(tm + T_D3, sbase + S_H, sbase + S_W3, 64, 64, 64, false); });
     if (abort) break;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    {
+      const int h = hh;
       float zr[16], zi[16], hr[16], hi[16];
       tc::ld16(tm + lo + T_D3 + 16 * h, zr);
       tc::ld16(tm + lo + T_D3 + 32 + 16 * h, zi);
@@ -280,15 +288,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
         hr[k] = amp * co;
         hi[k] = amp * s;
       }
-      st8(sm + S_H3, t, 16 * h, hr);
-      st8(sm + S_H3, t, 8 + 16 * h, hr + 8);
-      st8(sm + S_H3, t, 32 + 16 * h, hi);
-      st8(sm + S_H3, t, 40 + 16 * h, hi + 8);
+      st8(sm + S_H3, row, 16 * h, hr);
+      st8(sm + S_H3, row, 8 + 16 * h, hr + 8);
+      st8(sm + S_H3, row, 32 + 16 * h, hi);
+      st8(sm + S_H3, row, 40 + 16 * h, hi + 8);
     }
     // -- output layer ----------------------------------------------------------
     step([&] { gemm_act_w(tm + T_DO, sbase + S_H3, sbase + S_WO, 16, 16, 64, false); });
     if (abort) break;
-    {
+    if (hh == 0) {  // warp-uniform
       float d[16];
       tc::ld16(tm + lo + T_DO, d);
       if (a.y && valid) a.y[c] = make_float2(d[0] + par[P_BOR], d[1] + par[P_BOI]);
@@ -301,8 +309,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
       });
       if (abort) break;
       // G_z3 = conj(i w3 h3) G_h3 (h3 recomputed from z3 in TMEM)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      {
+        const int h = hh;
         float gr[16], gi[16], zr[16], zi[16];
         tc::ld16(tm + lo + T_DO + 16 * h, gr);
         tc::ld16(tm + lo + T_DO + 32 + 16 * h, gi);
@@ -319,16 +327,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
           zr[k] = w3 * (hr * gi[k] - hi * gr[k]);
           zi[k] = -w3 * (hr * gr[k] + hi * gi[k]);
         }
-        st8(sm + S_GZ, t, 16 * h, zr);
-        st8(sm + S_GZ, t, 8 + 16 * h, zr + 8);
-        st8(sm + S_GZ, t, 32 + 16 * h, zi);
-        st8(sm + S_GZ, t, 40 + 16 * h, zi + 8);
+        st8(sm + S_GZ, row, 16 * h, zr);
+        st8(sm + S_GZ, row, 8 + 16 * h, zr + 8);
+        st8(sm + S_GZ, row, 32 + 16 * h, zi);
+        st8(sm + S_GZ, row, 40 + 16 * h, zi + 8);
       }
       step([&] { gemm_act_wT(tm + T_D3, sbase + S_GZ, sbase + S_W3, 64, 64, 64); });
       if (abort) break;
       // G_z2
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      {
+        const int h = hh;
         float gr[16], gi[16], zr[16], zi[16];
         tc::ld16(tm + lo + T_D3 + 16 * h, gr);
         tc::ld16(tm + lo + T_D3 + 32 + 16 * h, gi);
@@ -345,16 +353,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
           zr[k] = w2 * (hr * gi[k] - hi * gr[k]);
           zi[k] = -w2 * (hr * gr[k] + hi * gi[k]);
         }
-        st8(sm + S_GZ, t, 64 + 16 * h, zr);
-        st8(sm + S_GZ, t, 72 + 16 * h, zr + 8);
-        st8(sm + S_GZ, t, 96 + 16 * h, zi);
-        st8(sm + S_GZ, t, 104 + 16 * h, zi + 8);
+        st8(sm + S_GZ, row, 64 + 16 * h, zr);
+        st8(sm + S_GZ, row, 72 + 16 * h, zr + 8);
+        st8(sm + S_GZ, row, 96 + 16 * h, zi);
+        st8(sm + S_GZ, row, 104 + 16 * h, zi + 8);
       }
       step([&] { gemm_act_wT(tm + T_D2, sbase + S_GZ + 8 * GRP, sbase + S_W2, 64, 64, 64); });
       if (abort) break;
       // G_z1 = Re(conj(G_h1) i w1 h1)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      {
+        const int h = hh;
         float gr[16], gi[16], z[16];
         tc::ld16(tm + lo + T_D2 + 16 * h, gr);
         tc::ld16(tm + lo + T_D2 + 32 + 16 * h, gi);
@@ -368,8 +376,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
           om1 += zz * q;
           z[k] = w1 * q;
         }
-        st8(sm + S_GZ1, t, 16 * h, z);
-        st8(sm + S_GZ1, t, 8 + 16 * h, z + 8);
+        st8(sm + S_GZ1, row, 16 * h, z);
+        st8(sm + S_GZ1, row, 8 + 16 * h, z + 8);
       }
       // G_x = W1^T G_z1 ; hidden / layer-1 weight-gradient accumulation
       step([&] {
@@ -379,8 +387,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
       });
       if (abort) break;
       if (a.gx) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        {
+          const int h = hh;
           float d[16];
           tc::ld16(tm + lo + T_D1 + 16 * h, d);
           if (valid) {
@@ -402,7 +410,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
     if (!abort) {
       // -- raw accumulators -> this CTA's partial --------------------------------
       float* P = a.part + size_t(blockIdx.x) * kPartFloats;
-      const int row = 32 * w + (t & 31);
       auto rd = [&](uint32_t col, float (&d)[16]) {
         if (first) {
 #pragma unroll
@@ -412,7 +419,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
         }
       };
       float d[16];
-      if (w < 2) {  // rows 0..63: W3 real form and b3
+      if (hh == 1) {
+        // the raw accumulators are read by warps 0..3 (one per lane quarter)
+      } else if (quarter < 2) {  // rows 0..63: W3 real form and b3
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           rd(T_ACC + 16 * q, d);
@@ -460,14 +469,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_cmlp(const Args a) {
       }
       if ((t & 31) == 0) {
         red[w] = om1;
-        red[4 + w] = om2;
-        red[8 + w] = om3;
+        red[8 + w] = om2;
+        red[16 + w] = om3;
       }
       __syncthreads();
       if (t == 0) {
-        P[R_OM + 0] = ((red[0] + red[1]) + red[2]) + red[3];
-        P[R_OM + 1] = ((red[4] + red[5]) + red[6]) + red[7];
-        P[R_OM + 2] = ((red[8] + red[9]) + red[10]) + red[11];
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          float s = 0.f;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) s += red[8 * l + i];  // warps in order
+          P[R_OM + l] = s;
+        }
       }
     }
   }
