@@ -2,8 +2,10 @@
 //
 // Replaces the accumulation that torch autograd performs for
 // `probe * object[tlY:brY, tlX:brX]` (Recovery.py:290, backward at :316):
-//   dO[window_b] += G_b * conj(P),   dP += G_b * conj(O[window_b]),
-// with G_b = dL/dpsi_b = (-1)^(x+y) E'_b (E'_b written by the fused kernel).
+//   dP += dL/dpsi_b conj(O[window_b]),   dO[window_b] += dL/dpsi_b conj(P),
+// with dL/dpsi_b = (-1)^(x+y) E'_b (E'_b written by the fused kernel).
+// k_dP_terms runs first: it reduces dP and turns E'_b in place into the
+// object-gradient terms G_b, which k_dO then only has to sum.
 // No floating-point atomics: every output element is owned by one thread
 // that sums its contributions in ascending pattern order; the dP group
 // partials are summed in group order by whichever block arrives last (an
@@ -14,10 +16,12 @@ namespace pty {
 
 PTY_DEVI float2 c_negif(float2 a, int odd) { return odd ? make_float2(-a.x, -a.y) : a; }
 
-// dO over one kTile x kTile canvas tile, 256 threads x kTile/8 rows.
-__global__ void __launch_bounds__(256) k_dO(const float2* __restrict__ Eb, const float2* __restrict__ P,
-                                            const int2* __restrict__ tlb, int B, int H, int W, int M,
-                                            int ntx, float2* __restrict__ dO, int accumulate) {
+// dO over one kTile x kTile canvas tile, 256 threads x kTile/8 rows: the
+// overlapping patterns are compacted in ascending order, then each thread sums
+// their terms G_b = dL/dpsi_b conj(P) at its 4 pixels (k_dP_terms wrote G_b).
+__global__ void __launch_bounds__(256) k_dO(const float2* __restrict__ Gb, const int2* __restrict__ tlb, int B,
+                                            int H, int W, int M, int ntx, float2* __restrict__ dO,
+                                            int accumulate) {
   __shared__ int list[256];
   __shared__ int wcnt[8];
   const int tile = blockIdx.x;
@@ -54,13 +58,12 @@ __global__ void __launch_bounds__(256) k_dO(const float2* __restrict__ Eb, const
         const int bb = list[i];
         const int2 c = __ldg(tlb + bb);
         const int lx = X - c.y;
-        const float2* Ep = Eb + size_t(bb) * M * M;
+        const float2* Gp = Gb + size_t(bb) * M * M;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
           const int ly = Y0 + 8 * j - c.x;
           c0[j] = make_float2(0.f, 0.f);
-          if (lx >= 0 && lx < M && ly >= 0 && ly < M)
-            c0[j] = c_negif(c_mulc(__ldg(Ep + ly * M + lx), __ldg(P + ly * M + lx)), (lx + ly) & 1);
+          if (lx >= 0 && lx < M && ly >= 0 && ly < M) c0[j] = __ldg(Gp + ly * M + lx);
         }
       }
       const bool two = i + 1 < n;
@@ -68,13 +71,12 @@ __global__ void __launch_bounds__(256) k_dO(const float2* __restrict__ Eb, const
         const int bb = list[i + 1];
         const int2 c = __ldg(tlb + bb);
         const int lx = X - c.y;
-        const float2* Ep = Eb + size_t(bb) * M * M;
+        const float2* Gp = Gb + size_t(bb) * M * M;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
           const int ly = Y0 + 8 * j - c.x;
           c1[j] = make_float2(0.f, 0.f);
-          if (lx >= 0 && lx < M && ly >= 0 && ly < M)
-            c1[j] = c_negif(c_mulc(__ldg(Ep + ly * M + lx), __ldg(P + ly * M + lx)), (lx + ly) & 1);
+          if (lx >= 0 && lx < M && ly >= 0 && ly < M) c1[j] = __ldg(Gp + ly * M + lx);
         }
       }
 #pragma unroll
@@ -115,68 +117,96 @@ __global__ void __launch_bounds__(256) k_loss_total(const double* __restrict__ l
   loss_sum_block(loss_pat, B, loss_total);
 }
 
-// dP: block (p, g) sums patterns [g*kGroup, (g+1)*kGroup) for kPixBlock probe
-// pixels; the last of the G blocks of pixel block p sums the partials in order.
-__global__ void __launch_bounds__(kPixBlock) k_dP(const float2* __restrict__ Eb, const float2* __restrict__ O,
-                                                  const int2* __restrict__ tlb, int B, int W, int M,
-                                                  float2* __restrict__ part, unsigned* __restrict__ done,
-                                                  float2* __restrict__ dP, int accumulate,
-                                                  const double* __restrict__ loss_pat,
-                                                  double* __restrict__ loss_total) {
+// Per-pattern gradient terms and dP.  Block (p, g) owns kPixBlock probe
+// pixels for the patterns [g*kGroup, (g+1)*kGroup); each (pattern, pixel)
+// pair is visited by exactly one thread, which
+//  * adds E'_b conj(O[window_b]) to its dP group partial (want_dP), and
+//  * overwrites E'_b in place with G_b = (-1)^(x+y) E'_b conj(P) (want_G), the
+//    object-gradient term k_dO then sums (the pixel's P is loaded once).
+// E' is read with ld.global.cg (it is rewritten in this kernel).  The last of
+// the G blocks of pixel block p sums the dP group partials in group order.
+__global__ void __launch_bounds__(kPixBlock) k_dP_terms(float2* __restrict__ Eb, const float2* __restrict__ O,
+                                                        const float2* __restrict__ P, const int2* __restrict__ tlb,
+                                                        int B, int W, int M, float2* __restrict__ part,
+                                                        unsigned* __restrict__ done, float2* __restrict__ dP,
+                                                        int want_G, int accumulate,
+                                                        const double* __restrict__ loss_pat,
+                                                        double* __restrict__ loss_total) {
   __shared__ int last;
   const int p = blockIdx.x, g = blockIdx.y, G = gridDim.y;
   const int idx = p * kPixBlock + threadIdx.x;
   const bool in = idx < M * M;
   const int y = idx / M, x = idx - (idx / M) * M;
+  const bool want_dP = dP != nullptr;
   if (in) {
+    const int odd = (x + y) & 1;
+    const float2 pc = want_G ? __ldg(P + idx) : make_float2(0.f, 0.f);
     float2 acc = make_float2(0.f, 0.f);
     const int b1 = min(B, (g + 1) * kGroup);
     int b = g * kGroup;
     for (; b + 1 < b1; b += 2) {  // two loads in flight, adds in order
       const int2 c0 = __ldg(tlb + b), c1 = __ldg(tlb + b + 1);
+      float2* e0p = Eb + size_t(b) * M * M + idx;
+      float2* e1p = Eb + size_t(b + 1) * M * M + idx;
+      float2 e0 = make_float2(0.f, 0.f), e1 = make_float2(0.f, 0.f);
       float2 t0 = make_float2(0.f, 0.f), t1 = make_float2(0.f, 0.f);
-      if (c0.x >= 0) t0 = c_mulc(__ldg(Eb + size_t(b) * M * M + idx), __ldg(O + size_t(c0.x + y) * W + c0.y + x));
-      if (c1.x >= 0)
-        t1 = c_mulc(__ldg(Eb + size_t(b + 1) * M * M + idx), __ldg(O + size_t(c1.x + y) * W + c1.y + x));
+      if (c0.x >= 0) {
+        e0 = __ldcg(e0p);
+        if (want_dP) t0 = c_mulc(e0, __ldg(O + size_t(c0.x + y) * W + c0.y + x));
+      }
+      if (c1.x >= 0) {
+        e1 = __ldcg(e1p);
+        if (want_dP) t1 = c_mulc(e1, __ldg(O + size_t(c1.x + y) * W + c1.y + x));
+      }
       acc = c_add(c_add(acc, t0), t1);
+      if (want_G) {
+        if (c0.x >= 0) __stcg(e0p, c_negif(c_mulc(e0, pc), odd));
+        if (c1.x >= 0) __stcg(e1p, c_negif(c_mulc(e1, pc), odd));
+      }
     }
     if (b < b1) {
       const int2 c0 = __ldg(tlb + b);
-      if (c0.x >= 0)
-        acc = c_add(acc, c_mulc(__ldg(Eb + size_t(b) * M * M + idx), __ldg(O + size_t(c0.x + y) * W + c0.y + x)));
+      if (c0.x >= 0) {
+        float2* e0p = Eb + size_t(b) * M * M + idx;
+        const float2 e0 = __ldcg(e0p);
+        if (want_dP) acc = c_add(acc, c_mulc(e0, __ldg(O + size_t(c0.x + y) * W + c0.y + x)));
+        if (want_G) __stcg(e0p, c_negif(c_mulc(e0, pc), odd));
+      }
     }
-    __stcg(reinterpret_cast<float2*>(part + size_t(g) * M * M + idx), c_negif(acc, (x + y) & 1));
+    if (want_dP) __stcg(reinterpret_cast<float2*>(part + size_t(g) * M * M + idx), c_negif(acc, odd));
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(done + p, 1u) == unsigned(G - 1));
-  __syncthreads();
-  if (last) {
+  if (want_dP) {  // uniform over the grid
     __threadfence();
-    if (in) {
-      float2 acc = make_float2(0.f, 0.f);
-      for (int gg = 0; gg < G; ++gg) acc = c_add(acc, __ldcg(part + size_t(gg) * M * M + idx));
-      dP[idx] = accumulate ? c_add(dP[idx], acc) : acc;
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(done + p, 1u) == unsigned(G - 1));
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      if (in) {
+        float2 acc = make_float2(0.f, 0.f);
+        for (int gg = 0; gg < G; ++gg) acc = c_add(acc, __ldcg(part + size_t(gg) * M * M + idx));
+        dP[idx] = accumulate ? c_add(dP[idx], acc) : acc;
+      }
+      if (threadIdx.x == 0) done[p] = 0u;  // ready for the next call
     }
-    if (threadIdx.x == 0) done[p] = 0u;  // ready for the next call
   }
   if (p == 0 && g == 0 && loss_total) loss_sum_block(loss_pat, B, loss_total);
 }
 
-int launch_assemble(const float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H,
-                    int W, int M, float2* dO, float2* dP, float2* part, unsigned* done,
-                    const double* loss_pat, double* loss_total, bool accumulate, cudaStream_t s) {
-  if (dO) {
-    const int ntx = (W + kTile - 1) / kTile, nty = (H + kTile - 1) / kTile;
-    k_dO<<<ntx * nty, 256, 0, s>>>(Eb, P, tlb, B, H, W, M, ntx, dO, accumulate ? 1 : 0);
-  }
-  if (dP) {
+int launch_assemble(float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W, int M,
+                    float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
+                    double* loss_total, bool accumulate, cudaStream_t s) {
+  if (dO || dP) {  // dP partials and, for dO, the in-place E' -> G conversion
     const int G = (B + kGroup - 1) / kGroup;
     dim3 grid(dp_counters(M), G);
-    k_dP<<<grid, kPixBlock, 0, s>>>(Eb, O, tlb, B, W, M, part, done, dP, accumulate ? 1 : 0, loss_pat,
-                                    loss_total);
+    k_dP_terms<<<grid, kPixBlock, 0, s>>>(Eb, O, P, tlb, B, W, M, part, done, dP, dO ? 1 : 0, accumulate ? 1 : 0,
+                                          loss_pat, loss_total);
   } else if (loss_total) {
     k_loss_total<<<1, 256, 0, s>>>(loss_pat, B, loss_total);
+  }
+  if (dO) {
+    const int ntx = (W + kTile - 1) / kTile, nty = (H + kTile - 1) / kTile;
+    k_dO<<<ntx * nty, 256, 0, s>>>(Eb, tlb, B, H, W, M, ntx, dO, accumulate ? 1 : 0);
   }
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }

@@ -11,11 +11,12 @@ constexpr int kPixBlock = 256;  // probe pixels per dP block
 // number of arrival counters the dP reduction needs (zeroed by the fused kernel)
 inline int dp_counters(int M) { return (M * M + kPixBlock - 1) / kPixBlock; }
 
-// dO (tile owner sums in ascending pattern order), dP (group partials, then the
-// last-arriving block sums them in group order) and the FP64 loss total; any
-// output may be null.  `done` holds dp_counters(M) zeroed counters.
-int launch_assemble(const float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H,
-                    int W, int M, float2* dO, float2* dP, float2* part, unsigned* done,
-                    const double* loss_pat, double* loss_total, bool accumulate, cudaStream_t s);
+// dP (group partials, then the last-arriving block sums them in group order),
+// dO (tile owner sums in ascending pattern order) and the FP64 loss total; any
+// output may be null.  E' is overwritten (with the object-gradient terms) when
+// dO is requested.  `done` holds dp_counters(M) zeroed counters.
+int launch_assemble(float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W, int M,
+                    float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
+                    double* loss_total, bool accumulate, cudaStream_t s);
 
 }  // namespace pty
