@@ -41,12 +41,15 @@ SIGNATURES = {
     "ptycho_hashgrid_segments": (_c_int, [_vp, _c_ll, _c_int, _vp, _vp]),
     "ptycho_hashgrid_backward": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp,
                                           _c_int, _vp]),
+    "ptycho_hashgrid_backward_planar": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float,
+                                                 _vp, _c_int, _vp]),
     "ptycho_cmlp_packed_bytes": (_c_size, []),
     "ptycho_cmlp_grad_floats": (_c_int, []),
     "ptycho_cmlp_pack": (_c_int, [_vp] * 12 + [_vp]),
     "ptycho_cmlp_forward": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp]),
     "ptycho_cmlp_backward_workspace_size": (_c_size, [_c_int]),
     "ptycho_cmlp_backward": (_c_int, [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _c_size, _vp, _vp]),
+    "ptycho_cmlp_backward_planar": (_c_int, [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _c_size, _vp, _vp]),
     "ptycho_adam_step": (_c_int, [_pp, _pp, _pp, _pp, ctypes.POINTER(_c_ll), _c_int, _c_int, _c_float, _c_float,
                                   _c_float, _c_float, _vp]),
     "ptycho_adam_step_dev": (_c_int, [_pp, _pp, _pp, _pp, ctypes.POINTER(_c_ll), _c_int, _vp, _vp, _c_float,

@@ -77,14 +77,17 @@ class _CmlpFn(torch.autograd.Function):
         dev = x.device
         N = x.shape[0]
         gy = gy.reshape(N).to(torch.complex64).contiguous()
-        gx = torch.empty((N, 32), dtype=torch.float32, device=dev) if ctx.needs_input_grad[0] else None
+        # gx is produced feature-major ([32, N]) and handed on as its [N, 32]
+        # transpose view: the hash-encoder backward reads that layout coalesced
+        gxT = torch.empty((32, N), dtype=torch.float32, device=dev) if ctx.needs_input_grad[0] else None
         grad = torch.empty(int(L.ptycho_cmlp_grad_floats()), dtype=torch.float32, device=dev)
         ws = torch.empty(int(L.ptycho_cmlp_backward_workspace_size(N)), dtype=torch.uint8, device=dev)
         st = device_status(dev)
-        _lib.check(L.ptycho_cmlp_backward(packed.data_ptr(), x.data_ptr(), gy.data_ptr(), N,
-                                          gx.data_ptr() if gx is not None else None, grad.data_ptr(), None,
-                                          ws.data_ptr(), ws.numel(), st.data_ptr(), _stream(dev)),
-                   "ptycho_cmlp_backward")
+        _lib.check(L.ptycho_cmlp_backward_planar(packed.data_ptr(), x.data_ptr(), gy.data_ptr(), N,
+                                                 gxT.data_ptr() if gxT is not None else None, grad.data_ptr(),
+                                                 None, ws.data_ptr(), ws.numel(), st.data_ptr(), _stream(dev)),
+                   "ptycho_cmlp_backward_planar")
+        gx = gxT.t() if gxT is not None else None
         cplx = lambda o, n: torch.view_as_complex(grad[o:o + 2 * n].view(-1, 2))  # noqa: E731
         g = [grad[0:1024].view(32, 32), grad[1024:1056], grad[1056:1057],
              cplx(1058, 1024).view(32, 32), cplx(3106, 32), grad[3170:3171],

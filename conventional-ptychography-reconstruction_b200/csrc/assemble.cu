@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256) k_loss_total(const double* __restrict__ l
 //    object-gradient term k_dO then sums (the pixel's P is loaded once).
 // E' is read with ld.global.cg (it is rewritten in this kernel).  The last of
 // the G blocks of pixel block p sums the dP group partials in group order.
-__global__ void __launch_bounds__(kPixBlock) k_dP_terms(float2* __restrict__ Eb, const float2* __restrict__ O,
+__global__ void __launch_bounds__(kPixBlock, 6) k_dP_terms(float2* __restrict__ Eb, const float2* __restrict__ O,
                                                         const float2* __restrict__ P, const int2* __restrict__ tlb,
                                                         int B, int W, int M, float2* __restrict__ part,
                                                         unsigned* __restrict__ done, float2* __restrict__ dP,
@@ -143,34 +143,25 @@ __global__ void __launch_bounds__(kPixBlock) k_dP_terms(float2* __restrict__ Eb,
     const float2 pc = want_G ? __ldg(P + idx) : make_float2(0.f, 0.f);
     float2 acc = make_float2(0.f, 0.f);
     const int b1 = min(B, (g + 1) * kGroup);
-    int b = g * kGroup;
-    for (; b + 1 < b1; b += 2) {  // two loads in flight, adds in order
-      const int2 c0 = __ldg(tlb + b), c1 = __ldg(tlb + b + 1);
-      float2* e0p = Eb + size_t(b) * M * M + idx;
-      float2* e1p = Eb + size_t(b + 1) * M * M + idx;
-      float2 e0 = make_float2(0.f, 0.f), e1 = make_float2(0.f, 0.f);
-      float2 t0 = make_float2(0.f, 0.f), t1 = make_float2(0.f, 0.f);
-      if (c0.x >= 0) {
-        e0 = __ldcg(e0p);
-        if (want_dP) t0 = c_mulc(e0, __ldg(O + size_t(c0.x + y) * W + c0.y + x));
+    constexpr int U = 4;  // patterns whose loads are in flight together
+    for (int b = g * kGroup; b < b1; b += U) {
+      float2 e[U], t[U];
+      bool ok[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const int2 c = b + k < b1 ? __ldg(tlb + b + k) : make_int2(-1, -1);
+        ok[k] = c.x >= 0;
+        e[k] = make_float2(0.f, 0.f);
+        t[k] = make_float2(0.f, 0.f);
+        if (ok[k]) {
+          e[k] = __ldcg(Eb + size_t(b + k) * M * M + idx);
+          if (want_dP) t[k] = c_mulc(e[k], __ldg(O + size_t(c.x + y) * W + c.y + x));
+        }
       }
-      if (c1.x >= 0) {
-        e1 = __ldcg(e1p);
-        if (want_dP) t1 = c_mulc(e1, __ldg(O + size_t(c1.x + y) * W + c1.y + x));
-      }
-      acc = c_add(c_add(acc, t0), t1);
-      if (want_G) {
-        if (c0.x >= 0) __stcg(e0p, c_negif(c_mulc(e0, pc), odd));
-        if (c1.x >= 0) __stcg(e1p, c_negif(c_mulc(e1, pc), odd));
-      }
-    }
-    if (b < b1) {
-      const int2 c0 = __ldg(tlb + b);
-      if (c0.x >= 0) {
-        float2* e0p = Eb + size_t(b) * M * M + idx;
-        const float2 e0 = __ldcg(e0p);
-        if (want_dP) acc = c_add(acc, c_mulc(e0, __ldg(O + size_t(c0.x + y) * W + c0.y + x)));
-        if (want_G) __stcg(e0p, c_negif(c_mulc(e0, pc), odd));
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        acc = c_add(acc, t[k]);  // ascending pattern order
+        if (want_G && ok[k]) __stcg(Eb + size_t(b + k) * M * M + idx, c_negif(c_mulc(e[k], pc), odd));
       }
     }
     if (want_dP) __stcg(reinterpret_cast<float2*>(part + size_t(g) * M * M + idx), c_negif(acc, odd));

@@ -141,9 +141,10 @@ struct Args {
   const float2* gy;  // [N]
   int N;
   float2* y;         // [N] or null
-  float* gx;         // [N][32] or null
+  float* gx;         // [N][32] (or [32][N] when gx_planar) or null
   float* part;       // [gridDim.x][kPartFloats]
   int32_t* status;
+  int gx_planar;     // gx feature-major: feature f of row c at gx[f * N + c]
 };
 
 template <bool BWD>
@@ -392,9 +393,14 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
           float d[16];
           tc::ld16(tm + lo + T_D1 + 16 * h, d);
           if (valid) {
-            float4* gp = reinterpret_cast<float4*>(a.gx + size_t(c) * 32 + 16 * h);
+            if (a.gx_planar) {  // per feature, a warp stores 32 consecutive rows
 #pragma unroll
-            for (int q = 0; q < 4; ++q) gp[q] = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
+              for (int i = 0; i < 16; ++i) a.gx[size_t(16 * h + i) * a.N + c] = d[i];
+            } else {
+              float4* gp = reinterpret_cast<float4*>(a.gx + size_t(c) * 32 + 16 * h);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) gp[q] = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
+            }
           }
         }
       }
@@ -662,7 +668,7 @@ size_t ptycho_cmlp_backward_workspace_size(int N) {
   return pty_align_up(size_t(parts > 0 ? parts : 1) * cm::kPartFloats * sizeof(float), 256);
 }
 
-int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, int N, float* gx, float* grad,
+static int cmlp_backward(int planar, const void* packed, const float* x, const float* gy, int N, float* gx, float* grad,
                          float* y, void* workspace, size_t workspace_bytes, int32_t* status_out,
                          ptycho_stream_t stream) {
   if (!packed || !grad || N < 0 || (N > 0 && (!x || !gy))) return PTYCHO_ERR_INVALID_ARG;
@@ -684,13 +690,25 @@ int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, in
     return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
   }
   cm::Args a{static_cast<const unsigned char*>(packed), x, reinterpret_cast<const float2*>(gy), N,
-             reinterpret_cast<float2*>(y), gx, static_cast<float*>(workspace), status_out};
+             reinterpret_cast<float2*>(y), gx, static_cast<float*>(workspace), status_out, planar};
   int grid = 0;
   int st = cm::launch<true>(a, s, &grid);
   if (st) return st;
   cm::k_cmlp_reduce<<<(cm::kGradFloats + 7) / 8, 256, 0, s>>>(static_cast<const float*>(workspace), grid,
                                                                   grad);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, int N, float* gx, float* grad,
+                         float* y, void* workspace, size_t workspace_bytes, int32_t* status_out,
+                         ptycho_stream_t stream) {
+  return cmlp_backward(0, packed, x, gy, N, gx, grad, y, workspace, workspace_bytes, status_out, stream);
+}
+
+int ptycho_cmlp_backward_planar(const void* packed, const float* x, const float* gy, int N, float* gx,
+                                float* grad, float* y, void* workspace, size_t workspace_bytes,
+                                int32_t* status_out, ptycho_stream_t stream) {
+  return cmlp_backward(1, packed, x, gy, N, gx, grad, y, workspace, workspace_bytes, status_out, stream);
 }
 
 }  // extern "C"

@@ -135,11 +135,22 @@ __global__ void __launch_bounds__(256) k_seg_starts(const int* __restrict__ skey
   for (int e = prev + 1; e <= cur; ++e) start[e] = int(i);
 }
 
+// feature gradient of a contribution: PLANAR = false -> item = n*L + l into
+// [N][L] float2; PLANAR = true -> item = 2*l*N + n into feature-major [2L][N]
+// floats (real part at item, imaginary part N further), which makes the
+// gathers of one entry's spatially adjacent coordinates coalesced
+template <bool PLANAR>
+PTY_DEVI float2 dfeat_at(const float* __restrict__ dfeat, int item, int N) {
+  if constexpr (PLANAR) return make_float2(__ldg(dfeat + item), __ldg(dfeat + item + N));
+  else return __ldg(reinterpret_cast<const float2*>(dfeat) + item);
+}
+
 // long segments (coarse levels): one warp per entry, lanes stride the segment
 // in order, fixed xor tree
+template <bool PLANAR>
 __global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ start, const int* __restrict__ item,
                                                        const float* __restrict__ weight,
-                                                       const float2* __restrict__ dfeat, int E,
+                                                       const float* __restrict__ dfeat, int N, int E,
                                                        float2* __restrict__ dtable, int accumulate) {
   const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -148,7 +159,7 @@ __global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ s
   float ax = 0.f, ay = 0.f;
   for (int j = s0 + lane; j < s1; j += 32) {
     const float w = __ldg(weight + j);
-    const float2 g = __ldg(dfeat + __ldg(item + j));
+    const float2 g = dfeat_at<PLANAR>(dfeat, __ldg(item + j), N);
     ax = fmaf(w, g.x, ax);
     ay = fmaf(w, g.y, ay);
   }
@@ -168,9 +179,10 @@ __global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ s
 }
 
 // short segments (fine levels): one thread per entry, sequential in order
+template <bool PLANAR>
 __global__ void __launch_bounds__(256) k_hash_bwd_thread(const int* __restrict__ start, const int* __restrict__ item,
                                                          const float* __restrict__ weight,
-                                                         const float2* __restrict__ dfeat, int e0, int E,
+                                                         const float* __restrict__ dfeat, int N, int e0, int E,
                                                          float2* __restrict__ dtable, int accumulate) {
   const int e = e0 + blockIdx.x * 256 + threadIdx.x;
   if (e >= E) return;
@@ -178,7 +190,7 @@ __global__ void __launch_bounds__(256) k_hash_bwd_thread(const int* __restrict__
   float ax = 0.f, ay = 0.f;
   for (int j = s0; j < s1; ++j) {
     const float w = __ldg(weight + j);
-    const float2 g = __ldg(dfeat + __ldg(item + j));
+    const float2 g = dfeat_at<PLANAR>(dfeat, __ldg(item + j), N);
     ax = fmaf(w, g.x, ax);
     ay = fmaf(w, g.y, ay);
   }
@@ -241,29 +253,51 @@ int ptycho_hashgrid_segments(const int32_t* sorted_key, long long K, int n_entri
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
-int ptycho_hashgrid_backward(const int32_t* start, const int32_t* item, const float* weight,
-                             const float* dfeatures, int N, int n_levels, int log2_hashmap_size,
-                             int base_resolution, float per_level_scale, float* dtable, int accumulate,
-                             ptycho_stream_t stream) {
+static int hash_backward(bool planar, const int32_t* start, const int32_t* item, const float* weight,
+                         const float* dfeatures, int N, int n_levels, int log2_hashmap_size, int base_resolution,
+                         float per_level_scale, float* dtable, int accumulate, ptycho_stream_t stream) {
   LevelTable L;
   int st = make_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scale, &L);
   if (st) return st;
   if (N < 0 || !start || !item || !weight || !dfeatures || !dtable) return PTYCHO_ERR_INVALID_ARG;
-  if (!pty_aligned(dfeatures, 8) || !pty_aligned(dtable, 8)) return PTYCHO_ERR_MISALIGNED;
+  if (!pty_aligned(dfeatures, planar ? 4 : 8) || !pty_aligned(dtable, 8)) return PTYCHO_ERR_MISALIGNED;
   // levels whose average segment is long go to the warp-per-entry kernel
   int split = 0;
   for (int l = 0; l < L.levels; ++l)
     if ((long long)N * 4 >= 16ll * L.n[l]) split = L.offset[l] + L.n[l];
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (split > 0)
-    k_hash_bwd_warp<<<(split + 7) / 8, 256, 0, s>>>(start, item, weight,
-                                                   reinterpret_cast<const float2*>(dfeatures), split,
-                                                   reinterpret_cast<float2*>(dtable), accumulate);
-  if (L.total > split)
-    k_hash_bwd_thread<<<(L.total - split + 255) / 256, 256, 0, s>>>(
-        start, item, weight, reinterpret_cast<const float2*>(dfeatures), split, L.total,
-        reinterpret_cast<float2*>(dtable), accumulate);
+  float2* dt = reinterpret_cast<float2*>(dtable);
+  if (split > 0) {
+    if (planar)
+      k_hash_bwd_warp<true><<<(split + 7) / 8, 256, 0, s>>>(start, item, weight, dfeatures, N, split, dt, accumulate);
+    else
+      k_hash_bwd_warp<false><<<(split + 7) / 8, 256, 0, s>>>(start, item, weight, dfeatures, N, split, dt, accumulate);
+  }
+  if (L.total > split) {
+    const unsigned g = (L.total - split + 255) / 256;
+    if (planar)
+      k_hash_bwd_thread<true><<<g, 256, 0, s>>>(start, item, weight, dfeatures, N, split, L.total, dt, accumulate);
+    else
+      k_hash_bwd_thread<false><<<g, 256, 0, s>>>(start, item, weight, dfeatures, N, split, L.total, dt, accumulate);
+  }
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+int ptycho_hashgrid_backward(const int32_t* start, const int32_t* item, const float* weight,
+                             const float* dfeatures, int N, int n_levels, int log2_hashmap_size,
+                             int base_resolution, float per_level_scale, float* dtable, int accumulate,
+                             ptycho_stream_t stream) {
+  return hash_backward(false, start, item, weight, dfeatures, N, n_levels, log2_hashmap_size, base_resolution,
+                       per_level_scale, dtable, accumulate, stream);
+}
+
+int ptycho_hashgrid_backward_planar(const int32_t* start, const int32_t* item_planar, const float* weight,
+                                    const float* dfeatures_planar, int N, int n_levels, int log2_hashmap_size,
+                                    int base_resolution, float per_level_scale, float* dtable, int accumulate,
+                                    ptycho_stream_t stream) {
+  if ((long long)2 * n_levels * N > 0x7fffffffll) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  return hash_backward(true, start, item_planar, weight, dfeatures_planar, N, n_levels, log2_hashmap_size,
+                       base_resolution, per_level_scale, dtable, accumulate, stream);
 }
 
 }  // extern "C"

@@ -38,6 +38,13 @@ class _CSR:
         skey, order = torch.sort(key, stable=True)  # one-time set-up, deterministic order
         self.item = item[order].contiguous()
         self.weight = weight[order].contiguous()
+        # the same items addressed into a feature-major [2L][N] gradient (2*l*N + n),
+        # for ptycho_hashgrid_backward_planar; the order is unchanged
+        self.n = N
+        self.item_planar = None
+        if 2 * n_levels * N < 2 ** 31:
+            it = self.item.long()
+            self.item_planar = (2 * (it % n_levels) * N + it // n_levels).to(torch.int32).contiguous()
         self.start = torch.empty(n_entries + 1, dtype=torch.int32, device=dev)
         _lib.check(L.ptycho_hashgrid_segments(skey.data_ptr(), K, n_entries, self.start.data_ptr(),
                                               _stream(dev)), "ptycho_hashgrid_segments")
@@ -60,11 +67,19 @@ class _HashFn(torch.autograd.Function):
         coords, = ctx.saved_tensors
         enc = ctx.enc
         csr = enc._csr_for(coords)
-        gout = gout.contiguous().float()
+        N = coords.shape[0]
         dtable = torch.empty(enc.n_entries * 2, dtype=torch.float32, device=coords.device)
+        if (csr.item_planar is not None and gout.dtype == torch.float32 and gout.dim() == 2 and N > 1
+                and gout.stride() == (1, N)):
+            # feature-major gradient (the MLP backward's planar output): coalesced gathers
+            _lib.check(_lib.lib().ptycho_hashgrid_backward_planar(
+                csr.start.data_ptr(), csr.item_planar.data_ptr(), csr.weight.data_ptr(), gout.data_ptr(), N,
+                *enc.cfg, dtable.data_ptr(), 0, _stream(coords.device)), "ptycho_hashgrid_backward_planar")
+            return None, dtable, None
+        gout = gout.contiguous().float()
         _lib.check(_lib.lib().ptycho_hashgrid_backward(
             csr.start.data_ptr(), csr.item.data_ptr(), csr.weight.data_ptr(), gout.data_ptr(),
-            coords.shape[0], *enc.cfg, dtable.data_ptr(), 0, _stream(coords.device)), "ptycho_hashgrid_backward")
+            N, *enc.cfg, dtable.data_ptr(), 0, _stream(coords.device)), "ptycho_hashgrid_backward")
         return None, dtable, None
 
 

@@ -153,6 +153,19 @@ int ptycho_hashgrid_backward(const int32_t* start, const int32_t* item, const fl
                              int base_resolution, float per_level_scale, float* dtable,
                              int accumulate, ptycho_stream_t stream);
 
+/* The same backward for a feature gradient stored feature-major: dfeatures_planar
+ * [n_levels*2][N] (feature f of coordinate n at f*N + n), the layout
+ * ptycho_cmlp_backward_planar writes.  item_planar holds 2*l*N + n for each
+ * item n*n_levels + l of the CSR (same order).  One entry's contributors are
+ * spatially adjacent coordinates, so in this layout their gradients are read
+ * with coalesced loads.  Results are bitwise those of ptycho_hashgrid_backward.
+ * 2*n_levels*N must fit in int32. */
+int ptycho_hashgrid_backward_planar(const int32_t* start, const int32_t* item_planar,
+                                    const float* weight, const float* dfeatures_planar, int N,
+                                    int n_levels, int log2_hashmap_size, int base_resolution,
+                                    float per_level_scale, float* dtable, int accumulate,
+                                    ptycho_stream_t stream);
+
 /* ---------------------------------------------------------------------- *
  * Complex-exponential MLP on the tensor cores (tcgen05, BF16 operands, FP32
  * accumulation).  Replaces ComplexMLP.net (models/complex_inr.py:6-82,
@@ -182,6 +195,12 @@ size_t ptycho_cmlp_backward_workspace_size(int N);
 int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, int N, float* gx,
                          float* grad, float* y, void* workspace, size_t workspace_bytes,
                          int32_t* status_out, ptycho_stream_t stream);
+
+/* ptycho_cmlp_backward with gx written feature-major, gx [32][N] (feature f of
+ * coordinate n at gx[f*N + n]), the layout ptycho_hashgrid_backward_planar reads. */
+int ptycho_cmlp_backward_planar(const void* packed, const float* x, const float* gy, int N, float* gx,
+                                float* grad, float* y, void* workspace, size_t workspace_bytes,
+                                int32_t* status_out, ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
  * Fused Adam step over up to 48 float32 tensors (torch.optim.Adam,

@@ -72,6 +72,44 @@ def test_hashgrid_forward_backward(pkg, cfg):
     assert torch.equal(g1, enc.params.grad)
 
 
+@pytest.mark.parametrize("cfg", HASH_CFGS[1:])
+def test_hashgrid_planar_backward_bitwise(pkg, cfg):
+    """The feature-major backward (the MLP's planar gradient) gives the same bits
+    as the [N][L*2] backward: same CSR order, only the gather layout differs."""
+    L, log2T, base, pls = cfg
+    dev = torch.device("cuda")
+    enc = pkg.Encoding(2, {"otype": "HashGrid", "n_levels": L, "n_features_per_level": 2,
+                           "log2_hashmap_size": log2T, "base_resolution": base, "per_level_scale": pls}).to(dev)
+    n = 160
+    g = (np.arange(n) + 0.5) / n
+    ct = torch.from_numpy(np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2).astype(np.float32)).to(dev)
+    N = ct.shape[0]
+    csr = enc._csr_for(ct)
+    gfeat = torch.randn(N, 2 * L, device=dev)
+    gT = gfeat.t().contiguous()  # [2L][N]
+    Lb = pkg.lib()
+    a = torch.empty(enc.n_entries * 2, device=dev)
+    b = torch.empty_like(a)
+    s = torch.cuda.current_stream().cuda_stream
+    pkg._lib.check(Lb.ptycho_hashgrid_backward(csr.start.data_ptr(), csr.item.data_ptr(), csr.weight.data_ptr(),
+                                               gfeat.data_ptr(), N, *enc.cfg, a.data_ptr(), 0, s), "std")
+    pkg._lib.check(Lb.ptycho_hashgrid_backward_planar(csr.start.data_ptr(), csr.item_planar.data_ptr(),
+                                                      csr.weight.data_ptr(), gT.data_ptr(), N, *enc.cfg,
+                                                      b.data_ptr(), 0, s), "planar")
+    assert torch.equal(a, b)
+    # end to end: encoder -> MLP backward hands the planar gradient on
+    mlp, _ = _mlp_from_golden(pkg, 0, dev)
+    gy = torch.randn(N, 1, dtype=torch.complex64, device=dev)
+    enc.zero_grad()
+    mlp.net(enc(ct)).backward(gy)
+    chained = enc.params.grad.clone()
+    fd = enc(ct).detach().requires_grad_(True)
+    mlp.net(fd).backward(gy)
+    enc.zero_grad()
+    enc(ct).backward(fd.grad.contiguous())
+    assert torch.equal(chained, enc.params.grad)
+
+
 def _mlp_from_golden(pkg, k, dev):
     g = golden("complex_mlp.npz")
     cfg = g[f"m{k}/cfg"]
