@@ -104,6 +104,13 @@ PTY_DEVI uint32_t mapa(uint32_t saddr, uint32_t rank) {
 PTY_DEVI void st_cluster(uint32_t addr, float v) {
   asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
 }
+PTY_DEVI void st_cluster_v2(uint32_t addr, float a, float b) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(a), "f"(b) : "memory");
+}
+PTY_DEVI void st_cluster_v4(uint32_t addr, float a, float b, float c, float d) {
+  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+               : "memory");
+}
 PTY_DEVI void st_cluster_u32(uint32_t addr, unsigned v) {
   asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
@@ -125,20 +132,61 @@ PTY_DEVI void exch_cluster(float2 (&v)[E], int t, int r, float* re, float* im, c
   // = (thread part) ^ (element part); the bases are indexed by the element part
   constexpr int SH = DIR == 0 ? 6 : 4;
   const int qs = (sy >> SH) & 3;
-  uint32_t rre[4], rim[4];
+  // a CTA's shared memory maps linearly into the cluster window, so the
+  // imaginary plane of rank q sits (S_IM - S_RE) bytes above its real plane
+  uint32_t rre[4];
 #pragma unroll
-  for (int qe = 0; qe < 4; ++qe) {
-    rre[qe] = mapa(smem_u32(re), uint32_t(qs ^ qe));
-    rim[qe] = mapa(smem_u32(im), uint32_t(qs ^ qe));
-  }
+  for (int qe = 0; qe < 4; ++qe) rre[qe] = mapa(smem_u32(re), uint32_t(qs ^ qe));
+  constexpr uint32_t IMOFF = uint32_t(S_IM - S_RE);
   cl.sync();  // every CTA is done reading its planes
-  static_for<E>([&](auto ec) {
-    constexpr int e = decltype(ec)::value;
-    constexpr int qe = (eoff_y<M, PS>(e) >> SH) & 3;
-    const int off = A.row + addr_row<PS, LD, e>() + (A.xr ^ addr_x<PS, LD, e>());
-    st_cluster(rre[qe] + 4u * uint32_t(off), v[e].x);
-    st_cluster(rim[qe] + 4u * uint32_t(off), v[e].y);
-  });
+  if constexpr (DIR == 0) {
+    // Pass 2 holds x bits 0-3 (element bits 0-3) and y6 (bit 4): the 16 values
+    // of one y6 half land in one aligned 16-float group of the destination
+    // row, at column (A.xr ^ j).  Reorder them by the lane's XOR mask with four
+    // conditional-swap stages, then write the group with 16-byte stores.
+    static_for<E>([&](auto ec) {
+      constexpr int e = decltype(ec)::value;
+      static_assert(addr_row<PS, LD, e>() == 0 && addr_x<PS, LD, e>() == (e & 15), "pass-2 element map");
+      static_assert(((eoff_y<M, PS>(e) >> SH) & 3) == (e >> 4), "pass-2 rank map");
+    });
+    const int pm = A.xr & 15;
+    static_for<4>([&](auto bc) {
+      constexpr int bit = 1 << decltype(bc)::value;
+      const bool sw = (pm & bit) != 0;
+      static_for<E>([&](auto ec) {
+        constexpr int j = decltype(ec)::value;
+        if constexpr ((j & bit) == 0) {
+          const float2 a = v[j], b = v[j | bit];
+          v[j] = sw ? b : a;
+          v[j | bit] = sw ? a : b;
+        }
+      });
+    });
+    const uint32_t grp = 4u * uint32_t(A.row + (A.xr & ~15));
+    static_for<8>([&](auto gc) {
+      constexpr int g = decltype(gc)::value;  // y6 half g / 4, floats 4 (g % 4) .. +3
+      constexpr int e0 = 4 * g;
+      const uint32_t a = rre[g >> 2] + grp + 16u * uint32_t(g & 3);
+      st_cluster_v4(a, v[e0].x, v[e0 + 1].x, v[e0 + 2].x, v[e0 + 3].x);
+      st_cluster_v4(a + IMOFF, v[e0].y, v[e0 + 1].y, v[e0 + 2].y, v[e0 + 3].y);
+    });
+  } else {
+    // Pass 3 holds y bits 2-5 (element bits 0-3) and x0 (bit 4): the values
+    // e and e + 16 are adjacent columns (A.xr ^ x0) of one destination row;
+    // order each pair by the lane's column bit 0 and write it with 8-byte stores.
+    static_for<16>([&](auto ec) {
+      constexpr int e = decltype(ec)::value;
+      static_assert(addr_x<PS, LD, e>() == 0 && addr_x<PS, LD, e + 16>() == 1, "pass-3 column map");
+      static_assert(addr_row<PS, LD, e + 16>() == addr_row<PS, LD, e>(), "pass-3 row map");
+      static_assert(((eoff_y<M, PS>(e + 16) >> SH) & 3) == ((eoff_y<M, PS>(e) >> SH) & 3), "pass-3 rank map");
+      constexpr int qe = (eoff_y<M, PS>(e) >> SH) & 3;
+      const bool sw = (A.xr & 1) != 0;
+      const float2 lo = sw ? v[e + 16] : v[e], hi = sw ? v[e] : v[e + 16];
+      const uint32_t a = rre[qe] + 4u * uint32_t(A.row + addr_row<PS, LD, e>() + (A.xr & ~1));
+      st_cluster_v2(a, lo.x, hi.x);
+      st_cluster_v2(a + IMOFF, lo.y, hi.y);
+    });
+  }
   cl.sync();  // all values have landed
   int dx, dy;
   pos_base<PD>(t, r, dx, dy);
