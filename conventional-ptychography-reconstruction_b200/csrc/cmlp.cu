@@ -16,7 +16,8 @@
 // layer's complex units, so the sin / cos / exp chains between two MMAs are
 // split over 8 warps.
 //
-// Backward (training): the kernel recomputes the forward of its tile, then
+// Backward (training): the kernel recomputes the forward of its tile (keeping
+// the FP32 h2, h3 in shared memory for the gradient steps), then
 //   G_h3 = Wo_r^T G_y,  G_z = conj(i w h) G_h (complex layers),
 //   G_z1 = Re(conj(G_h1) i w1 h1),  G_h(prev) = W_r^T G_z,  G_x = W1^T G_z1
 // on the tensor core, and accumulates the weight gradients
@@ -58,7 +59,10 @@ constexpr int S_GY = S_H3 + 10 * GRP;  // 2 groups: (G_yr, G_yi, 0, ...), zeros
 constexpr int S_GZ1 = S_GY + 2 * GRP;  // 4 groups: G_z1
 constexpr int S_GZ = S_GZ1 + 4 * GRP;  // 16 groups: G_z3 (8), G_z2 (8)
 constexpr int S_ACT_END = S_GZ + 16 * GRP;
-constexpr int kSmemBwd = S_ACT_END;  // 136352 bytes: one CTA per SM
+// FP32 h2, h3 of the tile (backward only): [layer][re, im][32 units][128 rows],
+// kept from the forward recompute for the layer-3 and layer-2 gradients
+constexpr int S_HF = S_ACT_END;
+constexpr int kSmemBwd = S_HF + 2 * 2 * 32 * 128 * 4;  // 201888 bytes: one CTA per SM
 constexpr int kSmemFwd = S_GY;       // 91264 bytes: the forward needs x, h, h3 only -> two CTAs per SM
 
 // every MMA footprint used below stays inside [0, S_ACT_END)
@@ -158,6 +162,8 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + S_TMEM);
   float* par = reinterpret_cast<float*>(sm + S_PAR);
   float* red = reinterpret_cast<float*>(sm + S_RED);
+  float* hf = reinterpret_cast<float*>(sm + S_HF);  // valid in the backward only
+  auto hfi = [&](int layer, int part, int unit) { return ((layer * 2 + part) * 32 + unit) * 128 + row; };
   constexpr uint32_t NCOLS = BWD ? kColsBwd : kColsFwd;
   const uint32_t sbase = tc::smem_addr(sm);
 
@@ -267,6 +273,10 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
         sincos_rr(w2 * r, &s, &co);
         hr[k] = amp * co;
         hi[k] = amp * s;
+        if constexpr (BWD) {
+          hf[hfi(0, 0, 16 * h + k)] = hr[k];
+          hf[hfi(0, 1, 16 * h + k)] = hi[k];
+        }
       }
       st8(sm + S_H, row, 16 * h, hr);
       st8(sm + S_H, row, 8 + 16 * h, hr + 8);
@@ -288,6 +298,10 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
         sincos_rr(w3 * r, &s, &co);
         hr[k] = amp * co;
         hi[k] = amp * s;
+        if constexpr (BWD) {
+          hf[hfi(1, 0, 16 * h + k)] = hr[k];
+          hf[hfi(1, 1, 16 * h + k)] = hi[k];
+        }
       }
       st8(sm + S_H3, row, 16 * h, hr);
       st8(sm + S_H3, row, 8 + 16 * h, hr + 8);
@@ -320,10 +334,7 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
           const float r = zr[k] + par[P_B3R + 16 * h + k], i = zi[k] + par[P_B3I + 16 * h + k];
-          const float amp = __expf(-w3 * i);
-          float s, co;
-          sincos_rr(w3 * r, &s, &co);
-          const float hr = amp * co, hi = amp * s;
+          const float hr = hf[hfi(1, 0, 16 * h + k)], hi = hf[hfi(1, 1, 16 * h + k)];  // h3 of this tile
           om3 += gi[k] * (r * hr - i * hi) - gr[k] * (r * hi + i * hr);
           zr[k] = w3 * (hr * gi[k] - hi * gr[k]);
           zi[k] = -w3 * (hr * gr[k] + hi * gi[k]);
@@ -346,10 +357,7 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
           const float r = zr[k] + par[P_B2R + 16 * h + k], i = zi[k] + par[P_B2I + 16 * h + k];
-          const float amp = __expf(-w2 * i);
-          float s, co;
-          sincos_rr(w2 * r, &s, &co);
-          const float hr = amp * co, hi = amp * s;
+          const float hr = hf[hfi(0, 0, 16 * h + k)], hi = hf[hfi(0, 1, 16 * h + k)];  // h2 of this tile
           om2 += gi[k] * (r * hr - i * hi) - gr[k] * (r * hi + i * hr);
           zr[k] = w2 * (hr * gi[k] - hi * gr[k]);
           zi[k] = -w2 * (hr * gr[k] + hi * gi[k]);
