@@ -61,11 +61,20 @@ static int make_levels(int n_levels, int log2_T, int base_res, float per_level_s
   return off < (1ll << 31) ? PTYCHO_OK : PTYCHO_ERR_INVALID_ARG;
 }
 
+// entry of corner (cx, cy) of level l: index mod n_l.  A hashed level has
+// n_l = 2^log2_hashmap_size (a mask); a dense level's index cx + cy*r is below
+// n_l except for corners on the far edge, which take the modulo.
 PTY_DEVI int corner_entry(const LevelTable& L, int l, int cx, int cy) {
+  const uint32_t n = uint32_t(L.n[l]);
   uint32_t e;
-  if (L.dense[l]) e = uint32_t(cx) + uint32_t(cy) * uint32_t(L.res[l]);
-  else e = uint32_t(cx) ^ (uint32_t(cy) * kPrimeY);
-  return L.offset[l] + int(e % uint32_t(L.n[l]));
+  if (L.dense[l]) {
+    e = uint32_t(cx) + uint32_t(cy) * uint32_t(L.res[l]);
+    if (e >= n) e %= n;
+  } else {
+    e = uint32_t(cx) ^ (uint32_t(cy) * kPrimeY);
+    e = (n & (n - 1)) == 0 ? (e & (n - 1)) : (e % n);
+  }
+  return L.offset[l] + int(e);
 }
 
 // one thread per coordinate, all levels: adjacent threads hold adjacent

@@ -39,19 +39,29 @@ PTY_DEVI double abs2(float2 p) { return double(p.x) * double(p.x) + double(p.y) 
 __global__ void __launch_bounds__(NT) k_probe_prep(const float2* __restrict__ P, int M, int N,
                                                    float2* __restrict__ out, double* __restrict__ state) {
   __shared__ double rs[MAXD], cs[MAXD];
+  __shared__ double cpart[NT];  // column partials of the row groups
   __shared__ double sh[4];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int y = w; y < M; y += 32) {  // row sums
+  for (int y = w; y < M; y += 32) {  // row sums: one warp per row, coalesced
     double s = 0.0;
     for (int x = lane; x < N; x += 32) s += abs2(__ldg(P + size_t(y) * N + x));
     s = warp_sum(s);
     if (lane == 0) rs[y] = s;
   }
-  for (int x = w; x < N; x += 32) {  // column sums
+  {  // column sums: thread (g, x) sums rows g, g + G, ... of column x (coalesced),
+     // then the G group partials of each column are added in group order
+    const int G = NT / N > 0 ? NT / N : 1;
+    const int t = threadIdx.x, x = t % N, g = t / N;
     double s = 0.0;
-    for (int y = lane; y < M; y += 32) s += abs2(__ldg(P + size_t(y) * N + x));
-    s = warp_sum(s);
-    if (lane == 0) cs[x] = s;
+    if (g < G)
+      for (int y = g; y < M; y += G) s += abs2(__ldg(P + size_t(y) * N + x));
+    if (g < G) cpart[g * N + x] = s;
+    __syncthreads();
+    for (int xx = t; xx < N; xx += NT) {
+      double c = 0.0;
+      for (int gg = 0; gg < G; ++gg) c += cpart[gg * N + xx];
+      cs[xx] = c;
+    }
   }
   __syncthreads();
   if (w == 0) {
