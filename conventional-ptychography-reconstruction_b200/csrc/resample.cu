@@ -18,8 +18,9 @@
 // g -> t [h s][w], column pass t -> x-gradient.
 //
 // Each CTA loads LINES lines into two shared-memory planes (re, im; one float
-// of padding every 32), runs radix-16 (then 8/4/2) Stockham passes -- natural
-// order in and out, each thread holding one or two 16-value slots in
+// of padding every 32), runs radix-8 or radix-16 Stockham passes (8- or
+// 16-value register slots; lines up to 1024 points use 8 for more threads) --
+// natural order in and out, each thread holding one or two slots in
 // registers, in place between barriers -- remaps the spectrum, runs the
 // inverse passes and writes the lines back.  Twiddles come from a per-CTA
 // table exp(-2 pi i k / LMAX) rounded from double-precision sincospi.
@@ -42,8 +43,11 @@ struct Cfg {
   // (32-byte segments) and 4096 values per CTA when lines are short
   static constexpr int LINES = COL ? cmax(4, 4096 / LMAX) : cmax(1, 2048 / LMAX);
   static constexpr int N = LINES * LMAX;            // values held by the CTA
-  static constexpr int NT = cmin(512, N / 16);      // threads: one 16-value slot each, or two
-  static constexpr int SPT = N / 16 / NT;           // slots per thread (1 or 2)
+  // values per register slot: 8 (radix-8 passes) for lines up to 1024 points,
+  // which doubles the threads of these small, latency-bound transforms
+  static constexpr int VPT = LMAX <= 1024 ? 8 : 16;
+  static constexpr int NT = cmin(512, N / VPT);     // threads: one slot each, or two
+  static constexpr int SPT = N / VPT / NT;          // slots per thread (1 or 2)
   static constexpr int PLANE = N + N / 32;          // padded plane length (floats)
   static constexpr size_t SMEM = size_t(2) * PLANE * 4 + size_t(LMAX) * 8;
   static_assert(SPT == 1 || SPT == 2, "slot count");
@@ -55,14 +59,14 @@ PTY_DEVI int pad(int i) { return i + (i >> 5); }
 // One Stockham pass of radix R over every line of length L: butterfly j of a
 // line reads j + r L/R, applies exp(-+2 pi i (j mod NS) r / (NS R)) and the
 // radix-R DFT, and writes (j / NS) NS R + (j mod NS) + r NS.
-template <int L, int R, int NS, bool INV, int LINES, int NT, int SPT, int LMAX>
+template <int L, int R, int NS, bool INV, int LINES, int NT, int SPT, int LMAX, int VPT>
 PTY_DEVI void stockham(float* re, float* im, const float2* __restrict__ tw, int t) {
   constexpr int BPL = L / R;              // butterflies per line
   constexpr int NB = LINES * BPL;         // butterflies in the CTA
-  constexpr int PER = 16 / R;             // butterflies per 16-value slot
+  constexpr int PER = VPT / R;            // butterflies per VPT-value slot
   constexpr int NSLOT = NB / PER;         // slots in use (<= SPT * NT)
   constexpr int TWS = LMAX / (NS * R);    // twiddle table stride
-  float2 v[SPT][16];
+  float2 v[SPT][VPT];
   int jj[SPT][PER], base[SPT][PER];
 #pragma unroll
   for (int q = 0; q < SPT; ++q) {
@@ -113,14 +117,14 @@ PTY_DEVI void stockham(float* re, float* im, const float2* __restrict__ tw, int 
   __syncthreads();
 }
 
-// all passes of a length-L transform: radix 16 while 16 divides the rest, then 8/4/2
-template <int L, bool INV, int LINES, int NT, int SPT, int LMAX, int NS = 1>
+// all passes of a length-L transform: radix VPT while it divides the rest, then smaller
+template <int L, bool INV, int LINES, int NT, int SPT, int LMAX, int VPT, int NS = 1>
 PTY_DEVI void fft_lines(float* re, float* im, const float2* tw, int t) {
   if constexpr (NS < L) {
     constexpr int REST = L / NS;
-    constexpr int R = REST >= 16 ? 16 : REST;
-    stockham<L, R, NS, INV, LINES, NT, SPT, LMAX>(re, im, tw, t);
-    fft_lines<L, INV, LINES, NT, SPT, LMAX, NS * R>(re, im, tw, t);
+    constexpr int R = REST >= VPT ? VPT : REST;
+    stockham<L, R, NS, INV, LINES, NT, SPT, LMAX, VPT>(re, im, tw, t);
+    fft_lines<L, INV, LINES, NT, SPT, LMAX, VPT, NS * R>(re, im, tw, t);
   }
 }
 
@@ -160,7 +164,7 @@ __global__ void __launch_bounds__(Cfg<L1, L2, COL>::NT) k_resample(const float2*
     im[i] = x.y;
   }
   __syncthreads();
-  fft_lines<L1, false, LINES, NT, C::SPT, LMAX>(re, im, tw, t);
+  fft_lines<L1, false, LINES, NT, C::SPT, LMAX, C::VPT>(re, im, tw, t);
   // spectrum remap: frequency f in [-n/2, n/2), n = min(L1, L2), from f mod L1 to f mod L2
   if constexpr (L2 > L1) {
     for (int idx = t; idx < LINES * (L1 / 2); idx += NT) {  // negative frequencies move up
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(Cfg<L1, L2, COL>::NT) k_resample(const float2*
     }
     __syncthreads();
   }
-  fft_lines<L2, true, LINES, NT, C::SPT, LMAX>(re, im, tw, t);
+  fft_lines<L2, true, LINES, NT, C::SPT, LMAX, C::VPT>(re, im, tw, t);
   for (int idx = t; idx < LINES * L2; idx += NT) {
     int l, k;
     if constexpr (COL) {
