@@ -37,6 +37,7 @@ SIGNATURES = {
     "ptycho_haar_sparsity_backward": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     "ptycho_hashgrid_entries": (_c_int, [_c_int, _c_int, _c_int, _c_float]),
     "ptycho_hashgrid_forward": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
+    "ptycho_hashgrid_forward_planar": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
     "ptycho_hashgrid_contrib": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp, _vp]),
     "ptycho_hashgrid_segments": (_c_int, [_vp, _c_ll, _c_int, _vp, _vp]),
     "ptycho_hashgrid_backward": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp,
@@ -47,6 +48,7 @@ SIGNATURES = {
     "ptycho_cmlp_grad_floats": (_c_int, []),
     "ptycho_cmlp_pack": (_c_int, [_vp] * 12 + [_vp]),
     "ptycho_cmlp_forward": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp]),
+    "ptycho_cmlp_forward_planar": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp]),
     "ptycho_cmlp_backward_workspace_size": (_c_size, [_c_int]),
     "ptycho_cmlp_backward": (_c_int, [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _c_size, _vp, _vp]),
     "ptycho_cmlp_backward_planar": (_c_int, [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _c_size, _vp, _vp]),

@@ -52,6 +52,12 @@ def _f32(t):
     return t.contiguous().float()
 
 
+def _is_planar(x: torch.Tensor) -> bool:
+    """[N, 32] float32 view of a feature-major [32, N] buffer (the encoder's output)."""
+    return (x.dim() == 2 and x.shape[1] == 32 and x.shape[0] > 1 and x.stride() == (1, x.shape[0])
+            and x.dtype == torch.float32)
+
+
 class _CmlpFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, *params):
@@ -64,8 +70,11 @@ class _CmlpFn(torch.autograd.Function):
         N = x.shape[0]
         y = torch.empty((N,), dtype=torch.complex64, device=dev)
         st = device_status(dev)
-        _lib.check(L.ptycho_cmlp_forward(packed.data_ptr(), x.data_ptr(), N, y.data_ptr(), st.data_ptr(),
-                                         _stream(dev)), "ptycho_cmlp_forward")
+        planar = _is_planar(x)
+        fwd = L.ptycho_cmlp_forward_planar if planar else L.ptycho_cmlp_forward
+        _lib.check(fwd(packed.data_ptr(), x.data_ptr(), N, y.data_ptr(), st.data_ptr(), _stream(dev)),
+                   "ptycho_cmlp_forward")
+        ctx.planar = planar
         ctx.save_for_backward(x, packed)
         ctx.shapes = [(p.shape, p.dtype) for p in params]
         return y.unsqueeze(1)
@@ -77,17 +86,25 @@ class _CmlpFn(torch.autograd.Function):
         dev = x.device
         N = x.shape[0]
         gy = gy.reshape(N).to(torch.complex64).contiguous()
-        # gx is produced feature-major ([32, N]) and handed on as its [N, 32]
-        # transpose view: the hash-encoder backward reads that layout coalesced
-        gxT = torch.empty((32, N), dtype=torch.float32, device=dev) if ctx.needs_input_grad[0] else None
         grad = torch.empty(int(L.ptycho_cmlp_grad_floats()), dtype=torch.float32, device=dev)
         ws = torch.empty(int(L.ptycho_cmlp_backward_workspace_size(N)), dtype=torch.uint8, device=dev)
         st = device_status(dev)
-        _lib.check(L.ptycho_cmlp_backward_planar(packed.data_ptr(), x.data_ptr(), gy.data_ptr(), N,
-                                                 gxT.data_ptr() if gxT is not None else None, grad.data_ptr(),
-                                                 None, ws.data_ptr(), ws.numel(), st.data_ptr(), _stream(dev)),
-                   "ptycho_cmlp_backward_planar")
-        gx = gxT.t() if gxT is not None else None
+        gx = None
+        if ctx.planar:
+            # features came feature-major from the encoder: gx goes back the same way
+            # ([32, N], handed on as its [N, 32] transpose view, read coalesced there)
+            gxT = torch.empty((32, N), dtype=torch.float32, device=dev) if ctx.needs_input_grad[0] else None
+            _lib.check(L.ptycho_cmlp_backward_planar(packed.data_ptr(), x.data_ptr(), gy.data_ptr(), N,
+                                                     gxT.data_ptr() if gxT is not None else None,
+                                                     grad.data_ptr(), None, ws.data_ptr(), ws.numel(),
+                                                     st.data_ptr(), _stream(dev)), "ptycho_cmlp_backward_planar")
+            gx = gxT.t() if gxT is not None else None
+        else:
+            gx = torch.empty((N, 32), dtype=torch.float32, device=dev) if ctx.needs_input_grad[0] else None
+            _lib.check(L.ptycho_cmlp_backward(packed.data_ptr(), x.data_ptr(), gy.data_ptr(), N,
+                                              gx.data_ptr() if gx is not None else None, grad.data_ptr(), None,
+                                              ws.data_ptr(), ws.numel(), st.data_ptr(), _stream(dev)),
+                       "ptycho_cmlp_backward")
         cplx = lambda o, n: torch.view_as_complex(grad[o:o + 2 * n].view(-1, 2))  # noqa: E731
         g = [grad[0:1024].view(32, 32), grad[1024:1056], grad[1056:1057],
              cplx(1058, 1024).view(32, 32), cplx(3106, 32), grad[3170:3171],
@@ -105,7 +122,10 @@ class _FusedSequential(nn.Sequential):
     def forward(self, x):  # noqa: D401
         if not x.is_cuda:
             raise ValueError("features must be a CUDA tensor (there is no CPU path)")
-        return _CmlpFn.apply(x.float().contiguous(), *_params(self))
+        x = x.float()
+        if not _is_planar(x):
+            x = x.contiguous()
+        return _CmlpFn.apply(x, *_params(self))
 
 
 class ComplexMLP(nn.Module):

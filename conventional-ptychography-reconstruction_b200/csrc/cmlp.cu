@@ -149,6 +149,7 @@ struct Args {
   float* part;       // [gridDim.x][kPartFloats]
   int32_t* status;
   int gx_planar;     // gx feature-major: feature f of row c at gx[f * N + c]
+  int x_planar;      // x feature-major: feature f of row c at x[f * N + c]
 };
 
 template <bool BWD>
@@ -224,14 +225,19 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
     // -- inputs: this half's 16 of the row's 32 features ------------------------
     {
       float xv[16];
-      const float4* xp = reinterpret_cast<const float4*>(a.x + size_t(valid ? c : 0) * 32 + 16 * hh);
+      if (a.x_planar) {  // per feature, a warp reads 32 consecutive rows
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const float4 v = valid ? __ldg(xp + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        xv[4 * q] = v.x;
-        xv[4 * q + 1] = v.y;
-        xv[4 * q + 2] = v.z;
-        xv[4 * q + 3] = v.w;
+        for (int i = 0; i < 16; ++i) xv[i] = valid ? __ldg(a.x + size_t(16 * hh + i) * a.N + c) : 0.f;
+      } else {
+        const float4* xp = reinterpret_cast<const float4*>(a.x + size_t(valid ? c : 0) * 32 + 16 * hh);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 v = valid ? __ldg(xp + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+          xv[4 * q] = v.x;
+          xv[4 * q + 1] = v.y;
+          xv[4 * q + 2] = v.z;
+          xv[4 * q + 3] = v.w;
+        }
       }
       st8(sm + S_X, row, 16 * hh, xv);
       st8(sm + S_X, row, 16 * hh + 8, xv + 8);
@@ -660,13 +666,24 @@ int ptycho_cmlp_pack(const float* W1, const float* b1, const float* omega1, cons
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
-int ptycho_cmlp_forward(const void* packed, const float* x, int N, float* y, int32_t* status_out,
+static int cmlp_forward(int planar, const void* packed, const float* x, int N, float* y, int32_t* status_out,
                         ptycho_stream_t stream) {
   if (!packed || N < 0 || (N > 0 && (!x || !y))) return PTYCHO_ERR_INVALID_ARG;
-  if (!pty_aligned(packed, 16) || !pty_aligned(x, 16) || !pty_aligned(y, 8)) return PTYCHO_ERR_MISALIGNED;
+  if (!pty_aligned(packed, 16) || !pty_aligned(x, planar ? 4 : 16) || !pty_aligned(y, 8))
+    return PTYCHO_ERR_MISALIGNED;
   cm::Args a{static_cast<const unsigned char*>(packed), x, nullptr, N, reinterpret_cast<float2*>(y), nullptr,
-             nullptr, status_out};
+             nullptr, status_out, 0, planar};
   return cm::launch<false>(a, reinterpret_cast<cudaStream_t>(stream), nullptr);
+}
+
+int ptycho_cmlp_forward(const void* packed, const float* x, int N, float* y, int32_t* status_out,
+                        ptycho_stream_t stream) {
+  return cmlp_forward(0, packed, x, N, y, status_out, stream);
+}
+
+int ptycho_cmlp_forward_planar(const void* packed, const float* x_planar, int N, float* y, int32_t* status_out,
+                               ptycho_stream_t stream) {
+  return cmlp_forward(1, packed, x_planar, N, y, status_out, stream);
 }
 
 size_t ptycho_cmlp_backward_workspace_size(int N) {
@@ -698,7 +715,7 @@ static int cmlp_backward(int planar, const void* packed, const float* x, const f
     return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
   }
   cm::Args a{static_cast<const unsigned char*>(packed), x, reinterpret_cast<const float2*>(gy), N,
-             reinterpret_cast<float2*>(y), gx, static_cast<float*>(workspace), status_out, planar};
+             reinterpret_cast<float2*>(y), gx, static_cast<float*>(workspace), status_out, planar, planar};
   int grid = 0;
   int st = cm::launch<true>(a, s, &grid);
   if (st) return st;

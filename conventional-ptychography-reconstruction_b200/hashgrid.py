@@ -54,13 +54,15 @@ class _HashFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coords, params, enc):
         N = coords.shape[0]
-        out = torch.empty((N, enc.n_output_dims), dtype=torch.float32, device=coords.device)
-        _lib.check(_lib.lib().ptycho_hashgrid_forward(coords.data_ptr(), N, params.data_ptr(), *enc.cfg,
-                                                      out.data_ptr(), _stream(coords.device)),
-                   "ptycho_hashgrid_forward")
+        # features are produced feature-major ([L*F, N], coalesced) and returned as
+        # the [N, L*F] transpose view; the MLP kernels read that layout directly
+        outT = torch.empty((enc.n_output_dims, N), dtype=torch.float32, device=coords.device)
+        _lib.check(_lib.lib().ptycho_hashgrid_forward_planar(coords.data_ptr(), N, params.data_ptr(), *enc.cfg,
+                                                             outT.data_ptr(), _stream(coords.device)),
+                   "ptycho_hashgrid_forward_planar")
         ctx.enc = enc
         ctx.save_for_backward(coords)
-        return out
+        return outT.t()
 
     @staticmethod
     def backward(ctx, gout):

@@ -132,6 +132,13 @@ int ptycho_hashgrid_forward(const float* coords, int N, const float* table, int 
                             int log2_hashmap_size, int base_resolution, float per_level_scale,
                             float* features, ptycho_stream_t stream);
 
+/* The same encoding written feature-major: features_planar [n_levels*2][N]
+ * (feature f of coordinate n at f*N + n).  One thread per (coordinate, level),
+ * coalesced stores; values bitwise those of ptycho_hashgrid_forward. */
+int ptycho_hashgrid_forward_planar(const float* coords, int N, const float* table, int n_levels,
+                                   int log2_hashmap_size, int base_resolution, float per_level_scale,
+                                   float* features_planar, ptycho_stream_t stream);
+
 /* Static contributions of fixed coordinates: for each (coordinate n,
  * level l, corner k), index i = (n*n_levels + l)*4 + k: key[i] = table entry,
  * item[i] = n*n_levels + l (feature pair), weight[i] = bilinear weight.
@@ -196,8 +203,15 @@ int ptycho_cmlp_backward(const void* packed, const float* x, const float* gy, in
                          float* grad, float* y, void* workspace, size_t workspace_bytes,
                          int32_t* status_out, ptycho_stream_t stream);
 
-/* ptycho_cmlp_backward with gx written feature-major, gx [32][N] (feature f of
- * coordinate n at gx[f*N + n]), the layout ptycho_hashgrid_backward_planar reads. */
+/* ptycho_cmlp_forward with x feature-major, x_planar [32][N] (feature f of
+ * coordinate n at x_planar[f*N + n]), the layout ptycho_hashgrid_forward_planar
+ * writes. */
+int ptycho_cmlp_forward_planar(const void* packed, const float* x_planar, int N, float* y,
+                               int32_t* status_out, ptycho_stream_t stream);
+
+/* ptycho_cmlp_backward with x and gx feature-major ([32][N], feature f of
+ * coordinate n at f*N + n): x as ptycho_hashgrid_forward_planar writes it, gx as
+ * ptycho_hashgrid_backward_planar reads it. */
 int ptycho_cmlp_backward_planar(const void* packed, const float* x, const float* gy, int N, float* gx,
                                 float* grad, float* y, void* workspace, size_t workspace_bytes,
                                 int32_t* status_out, ptycho_stream_t stream);

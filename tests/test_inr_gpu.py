@@ -110,6 +110,51 @@ def test_hashgrid_planar_backward_bitwise(pkg, cfg):
     assert torch.equal(chained, enc.params.grad)
 
 
+@pytest.mark.parametrize("cfg", HASH_CFGS)
+def test_hashgrid_planar_forward_bitwise(pkg, cfg):
+    """The feature-major forward writes the same bits as the [N][L*2] forward."""
+    L, log2T, base, pls = cfg
+    dev = torch.device("cuda")
+    enc = pkg.Encoding(2, {"otype": "HashGrid", "n_levels": L, "n_features_per_level": 2,
+                           "log2_hashmap_size": log2T, "base_resolution": base, "per_level_scale": pls}).to(dev)
+    with torch.no_grad():
+        enc.params.uniform_(-1, 1)
+    ct = torch.rand(5003, 2, device=dev)
+    N = ct.shape[0]
+    a = torch.empty(N, 2 * L, device=dev)
+    b = torch.empty(2 * L, N, device=dev)
+    Lb = pkg.lib()
+    s = torch.cuda.current_stream().cuda_stream
+    pkg._lib.check(Lb.ptycho_hashgrid_forward(ct.data_ptr(), N, enc.params.data_ptr(), *enc.cfg, a.data_ptr(), s), "f")
+    pkg._lib.check(Lb.ptycho_hashgrid_forward_planar(ct.data_ptr(), N, enc.params.data_ptr(), *enc.cfg,
+                                                     b.data_ptr(), s), "fp")
+    assert torch.equal(a, b.t())
+    assert torch.equal(enc(ct), a)  # the module returns the feature-major result as a view
+
+
+def test_cmlp_planar_input_bitwise(pkg):
+    """Feature-major features (the encoder's layout) give the same outputs and
+    gradients as the same features stored [N][32]."""
+    dev = torch.device("cuda")
+    mlp, _ = _mlp_from_golden(pkg, 0, dev)
+    N = 3000
+    xT = (torch.randn(32, N, device=dev) * 0.05)
+    x_planar = xT.t().requires_grad_(True)            # [N, 32] view, stride (1, N)
+    x_dense = xT.t().contiguous().requires_grad_(True)
+    gy = torch.randn(N, 1, dtype=torch.complex64, device=dev)
+    outs = []
+    for x in (x_planar, x_dense):
+        mlp.zero_grad()
+        y = mlp.net(x)
+        y.backward(gy)
+        outs.append((y.detach().clone(), x.grad.clone(), [p.grad.clone() for p in mlp.parameters()]))
+    assert x_planar.grad.stride() == (1, N) or x_planar.grad.is_contiguous()
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
+    for ga, gb in zip(outs[0][2], outs[1][2]):
+        assert torch.equal(ga, gb)
+
+
 def _mlp_from_golden(pkg, k, dev):
     g = golden("complex_mlp.npz")
     cfg = g[f"m{k}/cfg"]
