@@ -199,7 +199,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (fp32)",
             "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": _config(w, batch, args),
+            "config": _config(w, w.batch, args),
             "cpu_baseline": {"value": rate, "unit": "patterns/s", "cores": torch.get_num_threads(),
                              "kind": "port", "sample": sample},
             "e2e": {"value": rate, "unit": "patterns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -316,6 +316,7 @@ def run_ours(args):
             Pparam.grad = None
             loss = pkg.fused_loss(Oparam, Pparam, slots[k][1], slots[k][0], w.loss_type)
             loss.backward()
+            exchange.all_reduce(Oparam.grad, Pparam.grad)  # N > 1: the step's gradient exchange
             out_host.copy_(loss.detach(), non_blocking=True)
             consumed[k].record(s)
 
@@ -359,6 +360,7 @@ def run_ours(args):
             Pparam.grad = None
             loss = pkg.fused_loss(Oparam, Pparam, tl, stack, w.loss_type, batch=ids_dev)
             loss.backward()
+            exchange.all_reduce(Oparam.grad, Pparam.grad)  # N > 1: the step's gradient exchange
             out_host.copy_(loss.detach(), non_blocking=True)
 
         for i in range(args.warmup):
