@@ -66,7 +66,7 @@ class _HashFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, gout):
-        coords, = ctx.saved_tensors
+        coords, = ctx.saved_tensors  # raises if coords were modified in place after the forward
         enc = ctx.enc
         csr = enc._csr_for(coords)
         N = coords.shape[0]
@@ -110,14 +110,25 @@ class Encoding(torch.nn.Module):
         self.n_entries = n
         g = torch.Generator().manual_seed(seed)
         self.params = torch.nn.Parameter(torch.rand(n * 2, generator=g) * 2e-4 - 1e-4)
-        self._csr = {}
+        self._csr = []
 
     def _csr_for(self, coords: torch.Tensor) -> _CSR:
-        k = (coords.data_ptr(), tuple(coords.shape), coords.device)
-        csr = self._csr.get(k)
-        if csr is None:
-            csr = _CSR(coords, self.cfg, self.n_entries)
-            self._csr = {k: csr} if len(self._csr) > 4 else {**self._csr, k: csr}
+        """The static contribution CSR of ``coords``, cached per coordinate buffer.
+
+        An entry holds a reference to the coordinate tensor, so its memory cannot
+        be taken by another tensor while cached, and matches on address, shape,
+        strides and version counter (shared by aliases): new coordinates, or the
+        same buffer modified in place, get a fresh CSR.  Fixed coordinates (an
+        INR's pixel grid) build it once."""
+        key = (coords.data_ptr(), tuple(coords.shape), tuple(coords.stride()), coords.device)
+        for k, t, ver, csr in self._csr:
+            if k == key and t._version == ver and coords._version == ver:
+                return csr
+        csr = _CSR(coords, self.cfg, self.n_entries)
+        self._csr = self._csr[-3:] + [(key, coords, coords._version, csr)]
+        return csr
+        csr = _CSR(coords, self.cfg, self.n_entries)
+        self._csr = self._csr[-3:] + [(coords, coords._version, csr)]
         return csr
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:

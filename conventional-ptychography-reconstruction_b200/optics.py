@@ -199,7 +199,9 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
         dO = dP = None
     ws_bytes = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, M, B))
     if workspace is None:
-        workspace = _default_ws.setdefault(dev, FwdAdjWorkspace())
+        # one default workspace per (device, stream): calls on one stream are
+        # ordered, calls on different streams must not share scratch
+        workspace = _default_ws.setdefault((dev, _stream_handle(dev)), FwdAdjWorkspace())
     ws = workspace.get(ws_bytes, dev)
     st = device_status(dev)
     _lib.check(_lib.lib().ptycho_fwd_adj(

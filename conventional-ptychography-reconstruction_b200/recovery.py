@@ -180,7 +180,9 @@ class Trainer:
         buf = torch.arange(n, dtype=torch.int32, device=dev)
         # warm-up outside capture (CSR, workspaces, FFT plans, kernel attributes);
         # parameters and optimizer state are restored afterwards
-        params = [p for p in self.model.parameters()]
+        # only trainable parameters change; frozen ones (the INR's coordinate grids)
+        # are left untouched, so caches keyed on their version stay valid
+        params = [p for p in self.model.parameters() if p.requires_grad]
         saved = [p.detach().clone() for p in params]
         saved_opt = {k: (v["exp_avg"].clone(), v["exp_avg_sq"].clone()) for k, v in self.opt.state.items()
                      if "exp_avg" in v}

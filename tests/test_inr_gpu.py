@@ -155,6 +155,33 @@ def test_cmlp_planar_input_bitwise(pkg):
         assert torch.equal(ga, gb)
 
 
+def test_hashgrid_backward_follows_changed_coordinates(pkg):
+    """The static CSR is rebuilt when the coordinates change: in place, or as a
+    new tensor that may reuse the freed memory."""
+    L, log2T, base, pls = HASH_CFGS[0]
+    dev = torch.device("cuda")
+    enc = pkg.Encoding(2, {"otype": "HashGrid", "n_levels": L, "n_features_per_level": 2,
+                           "log2_hashmap_size": log2T, "base_resolution": base, "per_level_scale": pls}).to(dev)
+    levels = inr.hashgrid_levels(L, log2T, base, float(np.float32(pls)))
+
+    def check(ct):
+        gfeat = torch.randn(ct.shape[0], 2 * L, device=dev)
+        enc.params.grad = None
+        enc(ct).backward(gfeat)
+        ref = inr.hashgrid_backward(ct.cpu().numpy().astype(np.float64), gfeat.cpu().numpy(), levels,
+                                    enc.n_entries, fp32_positions=True)
+        assert rel_max(enc.params.grad.cpu().numpy(), ref) <= 1e-5
+
+    a = torch.rand(2000, 2, device=dev)
+    check(a)
+    with torch.no_grad():
+        a.copy_(torch.rand(2000, 2, device=dev))  # same tensor, new values
+    check(a)
+    del a
+    b = torch.rand(2000, 2, device=dev)  # a new tensor, possibly at the same address
+    check(b)
+
+
 def _mlp_from_golden(pkg, k, dev):
     g = golden("complex_mlp.npz")
     cfg = g[f"m{k}/cfg"]
