@@ -301,8 +301,12 @@ class _FusedLoss(torch.autograd.Function):
             return None, None, None, None, None, None
         dO, dP = ctx.saved_tensors
         s = g.to(torch.float32)
-        gO = dO * s if ctx.needs_input_grad[0] else None
-        gP = dP * s if ctx.needs_input_grad[1] else None
+        want = [t for t, n in ((dO, ctx.needs_input_grad[0]), (dP, ctx.needs_input_grad[1])) if n]
+        # one multi-tensor launch scales both gradients (real views, out of place)
+        scaled = iter(torch.view_as_complex(t) for t in
+                      torch._foreach_mul([torch.view_as_real(t) for t in want], s))
+        gO = next(scaled) if ctx.needs_input_grad[0] else None
+        gP = next(scaled) if ctx.needs_input_grad[1] else None
         return gO, gP, None, None, None, None
 
 
