@@ -439,6 +439,13 @@ def time_to_residual(args):
     P0 = torch.from_numpy(work["probe"].astype(np.complex64)).to(dev) * float(np.sqrt(M * M))
     pls = torch_inr.per_level_scale_for(512, 16, 16)
     out = {"metric": "time-to-residual (pixel-grid x1.1)", "workload": WORKLOADS_DESC["c2"], "frames": F}
+    gt = torch.from_numpy(work["obj"].astype(np.complex64)).to(dev)
+    box = pkg.accuracy.coverage_box(work["tlY"], work["tlX"], (M, M), tuple(gt.shape), 0.5)
+
+    @torch.no_grad()
+    def object_err(model):  # FP64 on the device, global phase (and complex factor) removed, coverage box
+        e = pkg.accuracy.object_error(model()[0].reshape(gt.shape).to(torch.complex64), gt, box)
+        return {"nrmse_phase": round(e["nrmse"], 5), "nrmse_scaled": round(e["nrmse_scaled"], 5)}
 
     def timed(trainer, max_epochs, max_s, target):
         hist, t_train, reached = [], 0.0, None
@@ -465,7 +472,8 @@ def time_to_residual(args):
     r_pg = min(h[2] for h in hist[-max(1, len(hist) // 10):])  # converged tail
     target = 1.1 * r_pg
     out["pixel_grid"] = {"epochs": len(hist), "seconds": round(t_pg, 3), "residual": r_pg,
-                         "history": hist[:: max(1, len(hist) // 10)]}
+                         "object_error": object_err(pg), "history": hist[:: max(1, len(hist) // 10)]}
+    out["object_error_box"] = list(box)
     out["target_residual"] = target
     cfg = dict(model_type="inr", downsample_factor=2, n_levels=16, log2_hashmap_size=18, base_resolution=16,
                per_level_scale=pls, first_omega_0=10.0, hidden_omega_0=1.0, trainable_omega0=True,
@@ -477,6 +485,7 @@ def time_to_residual(args):
     out["inr_b200_kernels"] = {"reached": reached is not None, "seconds_to_target": reached[1] if reached else None,
                                "epochs_to_target": reached[0] if reached else None,
                                "seconds": round(t_in, 3), "best_residual": min(h[2] for h in hist),
+                               "object_error": object_err(model),
                                "ms_per_minibatch": 1e3 * t_in / (len(hist) * -(-F // 10)),
                                "history": hist[:: max(1, len(hist) // 10)]}
 
@@ -507,8 +516,9 @@ def time_to_residual(args):
                 den += float(Im.sum())
             return num / den
 
-    hist, reached, t_ref = timed(RefTrainer(), args.inr_epochs, args.ref_cap_s, target)
-    out["inr_reference_torch"] = {"reached": reached is not None,
+    ref = RefTrainer()
+    hist, reached, t_ref = timed(ref, args.inr_epochs, args.ref_cap_s, target)
+    out["inr_reference_torch"] = {"reached": reached is not None, "object_error": object_err(ref.model),
                                   "seconds_to_target": reached[1] if reached else None,
                                   "epochs_to_target": reached[0] if reached else None,
                                   "seconds": round(t_ref, 3), "best_residual": min(h[2] for h in hist),
@@ -528,13 +538,15 @@ def ttr_summary(out):
     a, b, pg = out["inr_b200_kernels"], out["inr_reference_torch"], out["pixel_grid"]
     return {"metric": out["metric"], "workload": "c2 (1024^2 canvas, 128^2 probe, 784 frames, batch 10)",
             "unit": "s", "higher_is_better": False,
-            "pixel_grid": {"epochs": pg["epochs"], "seconds": pg["seconds"], "residual": pg["residual"]},
+            "pixel_grid": {"epochs": pg["epochs"], "seconds": pg["seconds"], "residual": pg["residual"],
+                           "object_error": pg["object_error"]},
             "target_residual": out["target_residual"],
             "inr_b200": {"seconds_to_target": a["seconds_to_target"], "epochs": a["epochs_to_target"],
-                         "ms_per_minibatch": a["ms_per_minibatch"]},
+                         "ms_per_minibatch": a["ms_per_minibatch"], "object_error": a["object_error"]},
             "inr_reference_torch_same_gpu": {"seconds_to_target": b["seconds_to_target"],
                                              "epochs": b["epochs_to_target"],
                                              "ms_per_minibatch": b["ms_per_minibatch"],
+                                             "object_error": b["object_error"],
                                              "note": "tiny-cuda-nn replaced by a torch HashGrid restatement"}}
 
 

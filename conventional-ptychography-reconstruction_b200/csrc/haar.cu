@@ -1,4 +1,5 @@
-// haar.cu -- Haar-wavelet sparsity of the object and its gradient.
+// haar.cu -- Haar-wavelet sparsity of the object and its gradient; object error
+// against ground truth after global-phase alignment (FP64).
 //
 // Replaces haar_wavelet_sparsity_loss (utils/loss.py:60-83), added to the
 // loss at Recovery.py:309-313 when sparsity_weight != 0: with the 2x2 blocks
@@ -114,6 +115,104 @@ int ptycho_haar_sparsity_backward(const float* img, int H, int W, const double* 
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   hr::k_haar_bwd<<<hr::grid_for(H, W), hr::NT, 0, s>>>(reinterpret_cast<const float2*>(img), H, W, grad_loss,
                                                         reinterpret_cast<float2*>(grad_img));
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+}  // extern "C"
+
+// ---- object error after global-phase alignment (FP64) ----------------------
+// Over the box [y0, y1) x [x0, x1) of recon R and ground truth T (both [H][W]
+// complex64): c = sum conj(R) T, nR = sum |R|^2, nT = sum |T|^2 in FP64 (fixed
+// per-thread ranges, per-CTA trees, CTA-order sum).  The phase exp(i a) with
+// a = arg(c) minimises ||R e^{ia} - T|| (resolve_global_phase,
+// scripts/compare_object_ssim.py:92-98), and then
+//   NRMSE = sqrt((nR + nT - 2 |c|) / nT).
+// With the least-squares complex factor g = c / nR (phase and the probe/object
+// scale ambiguity both removed), ||g R - T||^2 / nT = 1 - |c|^2 / (nR nT).
+// out[0] = NRMSE, out[1], out[2] = cos a, sin a, out[3] = |c|, out[4] = nR,
+// out[5] = nT, out[6] = sqrt(1 - |c|^2 / (nR nT)).
+namespace pty {
+namespace oe {
+
+constexpr int NT = 256, MAXG = 592;
+
+__global__ void __launch_bounds__(NT) k_obj_err_part(const float2* __restrict__ R, const float2* __restrict__ T,
+                                                     int W, int y0, int y1, int x0, int x1,
+                                                     double* __restrict__ part) {
+  __shared__ double red[4][NT / 32];
+  const int bw = x1 - x0;
+  const long long n = (long long)(y1 - y0) * bw;
+  double cr = 0.0, ci = 0.0, nr = 0.0, nt = 0.0;
+  for (long long q = (long long)blockIdx.x * NT + threadIdx.x; q < n; q += (long long)gridDim.x * NT) {
+    const int y = y0 + int(q / bw), x = x0 + int(q % bw);
+    const float2 r = __ldg(R + size_t(y) * W + x), t = __ldg(T + size_t(y) * W + x);
+    cr += double(r.x) * t.x + double(r.y) * t.y;  // Re(conj(r) t)
+    ci += double(r.x) * t.y - double(r.y) * t.x;  // Im(conj(r) t)
+    nr += double(r.x) * r.x + double(r.y) * r.y;
+    nt += double(t.x) * t.x + double(t.y) * t.y;
+  }
+  double v[4] = {cr, ci, nr, nt};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = 0.0;
+    for (int i = 0; i < NT / 32; ++i) s += red[threadIdx.x][i];
+    part[blockIdx.x * 4 + threadIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(32) k_obj_err_final(const double* __restrict__ part, int G, double* __restrict__ out) {
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < G; i += 32)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] += part[i * 4 + k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if (threadIdx.x == 0) {
+    const double mag = sqrt(v[0] * v[0] + v[1] * v[1]);
+    const double nt = v[3];
+    out[0] = nt > 0.0 ? sqrt(fmax(v[2] + nt - 2.0 * mag, 0.0) / nt) : 0.0;
+    out[1] = mag > 0.0 ? v[0] / mag : 1.0;
+    out[2] = mag > 0.0 ? v[1] / mag : 0.0;
+    out[3] = mag;
+    out[4] = v[2];
+    out[5] = nt;
+    out[6] = (v[2] > 0.0 && nt > 0.0) ? sqrt(fmax(1.0 - (mag / v[2]) * (mag / nt), 0.0)) : 1.0;
+  }
+}
+
+inline int grid_for(long long n) {
+  const long long g = (n + NT * 8 - 1) / (NT * 8);
+  return g < 1 ? 1 : (g > MAXG ? MAXG : int(g));
+}
+
+}  // namespace oe
+}  // namespace pty
+
+extern "C" {
+
+size_t ptycho_object_error_workspace_size(void) { return size_t(pty::oe::MAXG) * 4 * sizeof(double); }
+
+int ptycho_object_error(const float* recon, const float* truth, int H, int W, int y0, int y1, int x0, int x1,
+                        double* out, void* workspace, size_t workspace_bytes, ptycho_stream_t stream) {
+  if (!recon || !truth || !out || H <= 0 || W <= 0) return PTYCHO_ERR_INVALID_ARG;
+  if (y0 < 0 || x0 < 0 || y1 > H || x1 > W || y0 >= y1 || x0 >= x1) return PTYCHO_ERR_INVALID_ARG;
+  if (!workspace || workspace_bytes < ptycho_object_error_workspace_size()) return PTYCHO_ERR_WORKSPACE;
+  if (!pty_aligned(recon, 8) || !pty_aligned(truth, 8) || !pty_aligned(out, 8) || !pty_aligned(workspace, 8))
+    return PTYCHO_ERR_MISALIGNED;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int G = pty::oe::grid_for((long long)(y1 - y0) * (x1 - x0));
+  double* part = static_cast<double*>(workspace);
+  pty::oe::k_obj_err_part<<<G, pty::oe::NT, 0, s>>>(reinterpret_cast<const float2*>(recon),
+                                                    reinterpret_cast<const float2*>(truth), W, y0, y1, x0, x1, part);
+  pty::oe::k_obj_err_final<<<1, 32, 0, s>>>(part, G, out);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 

@@ -292,6 +292,24 @@ int ptycho_haar_sparsity_backward(const float* img, int H, int W, const double* 
                                   float* grad_img, ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Object error against ground truth after global-phase alignment, in FP64:
+ * over the box [y0, y1) x [x0, x1) of recon and truth ([H][W] complex64),
+ * c = sum conj(recon) truth, and with the phase a = arg(c) (the minimiser of
+ * ||recon e^{ia} - truth||: resolve_global_phase, scripts/compare_object_ssim.py:92-98),
+ *   out[0] = sqrt((sum|recon|^2 + sum|truth|^2 - 2|c|) / sum|truth|^2),
+ *   out[1..2] = cos a, sin a,  out[3] = |c|, out[4..5] = the two energies,
+ *   out[6] = sqrt(1 - |c|^2 / (sum|recon|^2 sum|truth|^2)), the error after the
+ *            least-squares complex factor (phase and scale ambiguity removed).
+ * out: 7 device doubles.  Fixed-order sums.  workspace:
+ * ptycho_object_error_workspace_size() bytes.
+ * ---------------------------------------------------------------------- */
+size_t ptycho_object_error_workspace_size(void);
+
+int ptycho_object_error(const float* recon, const float* truth, int H, int W, int y0, int y1, int x0,
+                        int x1, double* out, void* workspace, size_t workspace_bytes,
+                        ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
  * must not trigger an allocation's device synchronisation).  No counterpart

@@ -243,6 +243,42 @@ def resolve_global_phase(recon, gt):
     return recon * (inner / abs(inner))
 
 
+def object_error(recon, gt, box=None):
+    """(NRMSE after resolve_global_phase, NRMSE after the least-squares complex
+    factor) over box = (y0, y1, x0, x1); FP64 (compare_object_ssim.py:92-98)."""
+    r = np.asarray(recon, dtype=np.complex128)
+    g = np.asarray(gt, dtype=np.complex128)
+    if box is not None:
+        y0, y1, x0, x1 = box
+        r, g = r[y0:y1, x0:x1], g[y0:y1, x0:x1]
+    ng = float(np.vdot(g, g).real)
+    a = resolve_global_phase(r, g) - g
+    e_phase = float(np.sqrt(np.vdot(a, a).real / ng))
+    c = np.vdot(r, g)
+    nr = float(np.vdot(r, r).real)
+    gfac = c / nr if nr > 0 else 0.0
+    d = gfac * r - g
+    e_scaled = float(np.sqrt(np.vdot(d, d).real / ng))
+    return e_phase, e_scaled
+
+
+def coverage_box(tlY, tlX, probe_shape, canvas_shape, frac=0.5):
+    """scan_coverage_mask + high_coverage_bbox (compare_object_ssim.py:42-72) on
+    integer window corners: bbox of pixels covered >= ceil(frac * max) times."""
+    M, N = probe_shape
+    Hc, Wc = canvas_shape
+    cov = np.zeros((Hc, Wc), dtype=np.int32)
+    for y, x in zip(np.asarray(tlY).ravel(), np.asarray(tlX).ravel()):
+        y0, y1, x0, x1 = max(0, y), min(Hc, y + M), max(0, x), min(Wc, x + N)
+        if y1 > y0 and x1 > x0:
+            cov[y0:y1, x0:x1] += 1
+    thr = max(1, int(np.ceil(frac * cov.max())))
+    ys, xs = np.where(cov >= thr)
+    if ys.size == 0:
+        return 0, Hc, 0, Wc
+    return int(ys.min()), int(ys.max()) + 1, int(xs.min()), int(xs.max()) + 1
+
+
 def data_residual(I_model, Imeas):
     """R = sum (sqrt(I) - sqrt(Imeas))^2 / sum Imeas, FP64 over the stack."""
     I_model = np.asarray(I_model, dtype=np.float64)

@@ -93,6 +93,18 @@ def test_probe_prep_and_haar_validation_before_device_work():
     assert L.ptycho_haar_sparsity_backward(fake, 64, 65, fake, fake, None) == 2
 
 
+def test_object_error_validation_before_device_work():
+    L = load_pkg().lib()
+    fake = ctypes.c_void_p(4096)
+    n = L.ptycho_object_error_workspace_size()
+    assert n >= 4 * 8
+    assert L.ptycho_object_error(None, fake, 8, 8, 0, 8, 0, 8, fake, fake, n, None) == 1
+    assert L.ptycho_object_error(fake, fake, 8, 8, 0, 9, 0, 8, fake, fake, n, None) == 1  # box past the edge
+    assert L.ptycho_object_error(fake, fake, 8, 8, 4, 4, 0, 8, fake, fake, n, None) == 1  # empty box
+    assert L.ptycho_object_error(fake, fake, 8, 8, 0, 8, 0, 8, fake, fake, n - 8, None) == 4
+    assert L.ptycho_object_error(ctypes.c_void_p(4100), fake, 8, 8, 0, 8, 0, 8, fake, fake, n, None) == 3
+
+
 def test_workspace_size_monotone():
     L = load_pkg().lib()
     a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)
