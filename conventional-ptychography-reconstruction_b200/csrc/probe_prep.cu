@@ -36,15 +36,35 @@ PTY_DEVI double warp_sum(double v) {
 
 PTY_DEVI double abs2(float2 p) { return double(p.x) * double(p.x) + double(p.y) * double(p.y); }
 
+// Probes of up to kStageMax elements are first staged in shared memory (every
+// thread's loads independent, one memory round trip); the sums and the roll
+// then read shared memory, in the same order as the unstaged kernel, so both
+// give identical results.
+constexpr int kStageMax = 16384;
+
+template <bool STAGED>
 __global__ void __launch_bounds__(NT) k_probe_prep(const float2* __restrict__ P, int M, int N,
                                                    float2* __restrict__ out, double* __restrict__ state) {
   __shared__ double rs[MAXD], cs[MAXD];
   __shared__ double cpart[NT];  // column partials of the row groups
   __shared__ double sh[4];
+  extern __shared__ float2 sP[];  // STAGED: the probe, [M][N]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if constexpr (STAGED) {
+#pragma unroll
+    for (int k = 0; k < kStageMax / NT; ++k) {
+      const int idx = threadIdx.x + k * NT;
+      if (idx < M * N) sP[idx] = __ldg(P + idx);
+    }
+    __syncthreads();
+  }
+  auto ld = [&](int idx) -> float2 {
+    if constexpr (STAGED) return sP[idx];
+    else return __ldg(P + idx);
+  };
   for (int y = w; y < M; y += 32) {  // row sums: one warp per row, coalesced
     double s = 0.0;
-    for (int x = lane; x < N; x += 32) s += abs2(__ldg(P + size_t(y) * N + x));
+    for (int x = lane; x < N; x += 32) s += abs2(ld(y * N + x));
     s = warp_sum(s);
     if (lane == 0) rs[y] = s;
   }
@@ -54,7 +74,7 @@ __global__ void __launch_bounds__(NT) k_probe_prep(const float2* __restrict__ P,
     const int t = threadIdx.x, x = t % N, g = t / N;
     double s = 0.0;
     if (g < G)
-      for (int y = g; y < M; y += G) s += abs2(__ldg(P + size_t(y) * N + x));
+      for (int y = g; y < M; y += G) s += abs2(ld(y * N + x));
     if (g < G) cpart[g * N + x] = s;
     __syncthreads();
     for (int xx = t; xx < N; xx += NT) {
@@ -103,7 +123,7 @@ __global__ void __launch_bounds__(NT) k_probe_prep(const float2* __restrict__ P,
     int si = i + oy, sj = j + ox;
     si -= si >= M ? M : 0;
     sj -= sj >= N ? N : 0;
-    const float2 p = __ldg(P + size_t(si) * N + sj);
+    const float2 p = ld(si * N + sj);
     out[idx] = make_float2(p.x * k, p.y * k);
   }
 }
@@ -116,6 +136,7 @@ __global__ void __launch_bounds__(NT) k_probe_prep_bwd(const float2* __restrict_
   __shared__ double Sh;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double s = 0.0;
+#pragma unroll 8
   for (int idx = threadIdx.x; idx < M * N; idx += NT) {
     const float2 a = __ldg(g + idx), b = __ldg(Pout + idx);
     s += double(a.x) * double(b.x) + double(a.y) * double(b.y);  // Re(conj(G) P_out)
@@ -135,6 +156,7 @@ __global__ void __launch_bounds__(NT) k_probe_prep_bwd(const float2* __restrict_
   const bool norm = e > 0.0;
   const float k = float(state[2]);
   const float c = norm ? float(Sh / (double(M) * double(N))) : 0.f;
+#pragma unroll 8
   for (int idx = threadIdx.x; idx < M * N; idx += NT) {
     const int i = idx / N, j = idx - (idx / N) * N;
     int si = i + oy, sj = j + ox;
@@ -164,8 +186,23 @@ int ptycho_probe_center_normalize(const float* P, int M, int N, float* P_out, do
   if (P == P_out) return PTYCHO_ERR_INVALID_ARG;  // the roll reads P while P_out is written
   if (!pty_aligned(P, 8) || !pty_aligned(P_out, 8) || !pty_aligned(state, 8)) return PTYCHO_ERR_MISALIGNED;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  pp::k_probe_prep<<<1, pp::NT, 0, s>>>(reinterpret_cast<const float2*>(P), M, N,
-                                        reinterpret_cast<float2*>(P_out), state);
+  if (M * N <= pp::kStageMax) {
+    const int smem = M * N * int(sizeof(float2));
+    static bool attr_set[64] = {};  // per device: the dynamic shared-memory limit, once
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PTYCHO_ERR_LAUNCH;
+    if (!attr_set[dev]) {
+      if (cudaFuncSetAttribute(pp::k_probe_prep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               pp::kStageMax * int(sizeof(float2))) != cudaSuccess)
+        return PTYCHO_ERR_LAUNCH;
+      attr_set[dev] = true;
+    }
+    pp::k_probe_prep<true><<<1, pp::NT, smem, s>>>(reinterpret_cast<const float2*>(P), M, N,
+                                                   reinterpret_cast<float2*>(P_out), state);
+  } else {
+    pp::k_probe_prep<false><<<1, pp::NT, 0, s>>>(reinterpret_cast<const float2*>(P), M, N,
+                                                 reinterpret_cast<float2*>(P_out), state);
+  }
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
