@@ -592,6 +592,62 @@ def run_inr_step(args):
           flush=True)
 
 
+def run_gs(args):
+    """Gaussian-field rasteriser (the alternate object representation): one
+    step = forward render + backward of N Cholesky Gaussians onto a 512^2 grid
+    (the INR's 512^2 object grid for a 1024^2 canvas at downsample 2) through
+    the public autograd Function, sigma in [0.6, 3] px, max_patch_radius 16,
+    min_scale 0.5.  L2 flushed before every timed step; CUDA events."""
+    dev = torch.device("cuda")
+    pkg = importlib.import_module(PKG)
+    N, H, W = args.gs_gaussians, 512, 512
+    rng = np.random.default_rng(0)
+    xy = np.stack([rng.uniform(0, W - 1, N), rng.uniform(0, H - 1, N)], 1).astype(np.float32)
+    p1 = rng.uniform(np.log(0.6), np.log(3.0), (N, 2)).astype(np.float32)
+    p2 = rng.uniform(-1, 1, N).astype(np.float32)
+    wt = (0.05 * rng.standard_normal((N, 2))).astype(np.float32)
+    gout = torch.from_numpy(rng.standard_normal((2, H, W)).astype(np.float32)).to(dev)
+    leaves = [torch.from_numpy(a).to(dev).requires_grad_(True) for a in (xy, p1, p2, wt)]
+    fn = pkg.gsplat.GaussianRasterize2DCholesky
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def step():
+        for t in leaves:
+            t.grad = None
+        out = fn.apply(*leaves, H, W, 16, 0.5)
+        out.backward(gout)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream(dev)
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        step()
+        b.record(s)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = float(np.mean(times))
+    line = {"metric": "Gaussian-field render fwd+bwd", "value": N / (ms * 1e-3), "unit": "Gaussians/s",
+            "ms_per_step": ms, "steps": args.steps, "warmup": max(3, args.warmup), "higher_is_better": True,
+            "config": {"workload": f"{N} Cholesky Gaussians, 512^2 grid, sigma 0.6-3 px, 16x16 tiles",
+                       "l2": "flushed before every timed step"},
+            "gpu_launches_per_step": 5, "dtype": "f32", "data": "synthetic (seeded)"}
+    if not args.no_cpu_baseline:
+        from oracle import gsplat as og  # the CPU restatement, timed as the baseline only
+        n = min(N, 40000)
+        t0 = time.perf_counter()
+        og.render(og.CHOLESKY, xy[:n], p1[:n], p2[:n], wt[:n], H, W, 16, 0.5)
+        og.backward(og.CHOLESKY, xy[:n], p1[:n], p2[:n], wt[:n], H, W, 16, 0.5, gout.cpu().numpy())
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n / dt, "unit": "Gaussians/s", "cores": 1, "kind": "port",
+                                "sample": f"first {n} Gaussians of the same scene, NumPy restatement, fwd+bwd"}
+    print(json.dumps(line), flush=True)
+
+
 WORKLOADS_DESC = {"c2": "c2: 1024^2 canvas, 128^2 probe, 28x28 raster (784 frames), smooth_L1, batch 10; INR "
                         "16 levels x 2, log2 T 18, base 16, finest 512, 512^2 object grid (ds 2), MLP 64x2, "
                         "omega 10/1, probe initProbe + residual"}
@@ -614,12 +670,17 @@ def main():
     ap.add_argument("--inr-cap-s", type=float, default=60.0)
     ap.add_argument("--ref-cap-s", type=float, default=90.0)
     ap.add_argument("--no-ttr", action="store_true", help="omit the time-to-residual object from the bench line")
+    ap.add_argument("--gs", action="store_true", help="time the Gaussian-field rasteriser instead")
+    ap.add_argument("--gs-gaussians", type=int, default=100000)
     args = ap.parse_args()
     if args.time_to_residual:
         run_time_to_residual(args)
         return
     if args.inr_step:
         run_inr_step(args)
+        return
+    if args.gs:
+        run_gs(args)
         return
     if args.warmup < 3:
         args.warmup = 3

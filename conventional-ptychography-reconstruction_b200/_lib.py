@@ -38,6 +38,11 @@ SIGNATURES = {
     "ptycho_object_error_workspace_size": (_c_size, []),
     "ptycho_object_error": (_c_int, [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_size,
                                      _vp]),
+    "ptycho_gs_workspace_size": (_c_size, [_c_int, _c_int, _c_int]),
+    "ptycho_gs_forward": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp,
+                                   _vp, _c_size, _vp]),
+    "ptycho_gs_backward": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp,
+                                    _c_size, _vp, _vp, _vp, _vp, _vp]),
     "ptycho_hashgrid_entries": (_c_int, [_c_int, _c_int, _c_int, _c_float]),
     "ptycho_hashgrid_forward": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
     "ptycho_hashgrid_forward_planar": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),

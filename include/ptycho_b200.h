@@ -310,6 +310,39 @@ int ptycho_object_error(const float* recon, const float* truth, int H, int W, in
                         ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * 2-D complex Gaussian splatting (the Gaussian-field representation's
+ * rasteriser).  Replaces the gscp extension: GaussianRasterize2D /
+ * GaussianRasterize2DCholesky (gscp/cuda/_wrapper.py:18-163), i.e.
+ * rasterize_forward[_cholesky] / rasterize_backward[_cholesky]
+ * (gscp/csrc/rasterize_gaussians.cu, gscp_rasterizer/forward.cu, backward.cu).
+ *
+ * kind PTYCHO_GS_RS:       p1 = log scales [N][2], p2 = rotation [N] (radians)
+ * kind PTYCHO_GS_CHOLESKY: p1 = log diag(L) [N][2], p2 = L21 [N]
+ * xy [N][2] pixel positions (x, y), weight [N][2] (re, im); out [2][H][W].
+ * Per pixel: sum over the Gaussians whose 16x16-tile rectangle (3-sigma radius,
+ * clamped scales in [min_scale, max_patch_radius]) covers the pixel's tile,
+ * in ascending index, of weight * exp(power), terms with power > 0 or
+ * exp(power) < 1e-7 skipped -- the reference's semantics.  radii_out (int32
+ * [N], optional) receives the radii (0 = culled).  No host synchronisation;
+ * the workspace (ptycho_gs_workspace_size bytes, 256-byte aligned) carries the
+ * per-Gaussian geometry and the per-tile bitmasks from the forward to the
+ * backward, which must see the same inputs.  The backward writes every
+ * gradient (zeros for culled Gaussians) with fixed-order sums: deterministic.
+ * ---------------------------------------------------------------------- */
+enum { PTYCHO_GS_RS = 0, PTYCHO_GS_CHOLESKY = 1 };
+
+size_t ptycho_gs_workspace_size(int N, int H, int W);
+
+int ptycho_gs_forward(int kind, const float* xy, const float* p1, const float* p2, const float* weight,
+                      int N, int H, int W, int max_patch_radius, float min_scale, float* out,
+                      int* radii_out, void* workspace, size_t workspace_bytes, ptycho_stream_t stream);
+
+int ptycho_gs_backward(int kind, const float* xy, const float* p1, const float* p2, const float* weight,
+                       int N, int H, int W, int max_patch_radius, float min_scale, const float* grad_out,
+                       const void* workspace, size_t workspace_bytes, float* dxy, float* dp1, float* dp2,
+                       float* dweight, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
  * must not trigger an allocation's device synchronisation).  No counterpart

@@ -105,6 +105,22 @@ def test_object_error_validation_before_device_work():
     assert L.ptycho_object_error(ctypes.c_void_p(4100), fake, 8, 8, 0, 8, 0, 8, fake, fake, n, None) == 3
 
 
+def test_gsplat_validation_before_device_work():
+    L = load_pkg().lib()
+    fake = ctypes.c_void_p(4096)
+    assert L.ptycho_gs_workspace_size(0, 16, 16) == 0  # nothing to keep for no Gaussians
+    assert L.ptycho_gs_workspace_size(10, 0, 16) == 0
+    n = L.ptycho_gs_workspace_size(100, 64, 64)
+    args = (fake, fake, fake, fake, 100, 64, 64, 16, ctypes.c_float(0.5), fake, None, fake, n, None)
+    assert L.ptycho_gs_forward(2, *args) == 1  # unknown parameterisation
+    assert L.ptycho_gs_forward(0, fake, fake, fake, fake, 100, 64, 64, 0, ctypes.c_float(0.5), fake, None, fake, n,
+                               None) == 1  # max_patch_radius 0
+    assert L.ptycho_gs_forward(0, *args[:-3], fake, n - 256, None) == 4
+    assert L.ptycho_gs_forward(0, ctypes.c_void_p(4100), *args[1:]) == 3
+    assert L.ptycho_gs_backward(0, fake, fake, fake, fake, 100, 64, 64, 16, ctypes.c_float(0.5), None, fake, n,
+                                fake, fake, fake, fake, None) == 1
+
+
 def test_workspace_size_monotone():
     L = load_pkg().lib()
     a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)
