@@ -5,8 +5,10 @@
 // preprocessCUDA / preprocessCUDA_cholesky forward.cu:18-170, renderCUDA
 // forward.cu:175-250, renderCUDA_backward backward.cu:21-133 and the
 // preprocess backward passes backward.cu:138-275), bound to Python by
-// gscp/cuda/_wrapper.py:18-163.  Same per-Gaussian and per-pixel arithmetic;
-// the pipeline around it is different:
+// gscp/cuda/_wrapper.py:18-163.  Same per-Gaussian arithmetic and the same
+// per-pixel terms and skip rules (the exponent regrouped so pixels of one column
+// share work, equal up to rounding; exp is __expf, which the reference's
+// fast-math build also evaluates); the pipeline around it is different:
 //
 // * Binning without a sort or a host round trip.  The reference counts
 //   tile overlaps, scans them, reads the total back to the host, duplicates
@@ -16,10 +18,13 @@
 //   second-level mask marks the non-empty 32-bit words.  A tile reads its
 //   masks in index order, so its list comes out ascending with no sort, the
 //   whole forward is stream-ordered (graph-capturable) and needs no host sync.
-// * Render: one CTA per tile, one thread per pixel; the tile's list is
-//   compacted from the masks 8192 Gaussians at a time (block scan of the
-//   word popcounts) and the Gaussians are staged through shared memory 256 at
+// * Render: one CTA of 128 threads per tile, two pixels per thread (rows y and
+//   y + 8 of one column, sharing the Gaussian's column terms); the tile's list
+//   is compacted from the masks 4096 Gaussians at a time (block scan of the
+//   word popcounts) and the Gaussians are staged through shared memory 128 at
 //   a time.  Each pixel sums in ascending Gaussian index, as the reference.
+//   (Four pixels per thread in 64-thread CTAs measured slower: 1024 tiles
+//   then leave too few warps per SM.)
 // * Backward: one warp per Gaussian walks the tiles of its rectangle and sums
 //   its seven per-pixel terms in a fixed order (lane-strided pixels, then an
 //   XOR tree), then applies the preprocess chain rule.  No float atomics: the
@@ -37,7 +42,7 @@
 namespace pty {
 namespace gs {
 
-constexpr int TILE = 16, NPIX = TILE * TILE, CHUNK_WORDS = 256, WARPS_BWD = 8;
+constexpr int TILE = 16, NPIX = TILE * TILE, NTR = 128, CHUNK_WORDS = NTR, WARPS_BWD = 8;
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -150,22 +155,42 @@ __global__ void __launch_bounds__(256) k_gs_pre(const float* __restrict__ xy, co
     }
 }
 
-// One CTA per tile, one thread per pixel.
-__global__ void __launch_bounds__(NPIX) k_gs_render(const float2* __restrict__ weight, int H, int W, int tx, int NW,
-                                                    int NV, Geom g, float* __restrict__ out) {
+// Per-pixel exponent of one Gaussian, rearranged so a thread's two pixels
+// (one column, rows dy apart) share the column terms:
+//   power = -0.5 (cx dx^2 + cz dy^2) - cy dx dy = p0 - dy (0.5 cz dy + cy dx),
+// p0 = -0.5 cx dx^2.  The term is kept where power <= 0 and exp(power) >= 1e-7
+// (a select, so the warp does not diverge); exp is __expf, the exponential the
+// reference's fast-math build evaluates.
+PTY_DEVI float gauss_term(float p0, float h, float czh, float dy) {
+  const float power = fmaf(-dy, fmaf(czh, dy, h), p0);
+  const float G = __expf(power);
+  return (power <= 0.f && G >= 1e-7f) ? G : 0.f;
+}
+
+// One CTA of NTR threads per tile; thread (x, y) owns the pixels
+// (x, y + RSTEP r), r < ROWS, which share the Gaussian's column terms.
+__global__ void __launch_bounds__(NTR) k_gs_render(const float2* __restrict__ weight, int H, int W, int tx, int NW,
+                                                   int NV, Geom g, float* __restrict__ out) {
+  constexpr int ROWS = NPIX / NTR, RSTEP = TILE / ROWS;
   __shared__ int s_ids[CHUNK_WORDS * 32];
-  __shared__ float2 s_mean[NPIX];
-  __shared__ float4 s_con[NPIX];
-  __shared__ float2 s_w[NPIX];
-  __shared__ int s_warp[NPIX / 32];
+  __shared__ float2 s_mean[NTR];
+  __shared__ float4 s_con[NTR];  // (0.5 cx, cy, 0.5 cz, unused)
+  __shared__ float2 s_w[NTR];
+  __shared__ int s_warp[NTR / 32];
   const int t = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int px = (t % tx) * TILE + (threadIdx.x & (TILE - 1)), py = (t / tx) * TILE + (threadIdx.x / TILE);
-  const bool inside = px < W && py < H;
-  const float pxf = float(px), pyf = float(py);
+  const int px = (t % tx) * TILE + (threadIdx.x & (TILE - 1));
+  const int py = (t / tx) * TILE + (threadIdx.x / TILE);
+  const float pxf = float(px);
+  float pyf[ROWS], acc_re[ROWS], acc_im[ROWS];
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) {
+    pyf[r] = float(py + RSTEP * r);
+    acc_re[r] = 0.f;
+    acc_im[r] = 0.f;
+  }
   const uint32_t* m1 = g.mask1 + size_t(t) * NW;
   const uint32_t* m2 = g.mask2 + size_t(t) * NV;
-  float c0 = 0.f, c1 = 0.f;
   for (int w0 = 0; w0 < NW; w0 += CHUNK_WORDS) {
     const int w = w0 + threadIdx.x;
     uint32_t bits = 0;
@@ -182,7 +207,7 @@ __global__ void __launch_bounds__(NPIX) k_gs_render(const float2* __restrict__ w
     __syncthreads();
     int base = 0, total = 0;
 #pragma unroll
-    for (int k = 0; k < NPIX / 32; ++k) {
+    for (int k = 0; k < NTR / 32; ++k) {
       const int v = s_warp[k];
       base += k < wid ? v : 0;
       total += v;
@@ -193,36 +218,41 @@ __global__ void __launch_bounds__(NPIX) k_gs_render(const float2* __restrict__ w
       bits &= bits - 1;
     }
     __syncthreads();
-    for (int b0 = 0; b0 < total; b0 += NPIX) {
-      const int j = b0 + threadIdx.x;
+    for (int c0 = 0; c0 < total; c0 += NTR) {
+      const int j = c0 + threadIdx.x;
       if (j < total) {
         const int id = s_ids[j];
+        const float4 con = g.conic[id];
         s_mean[threadIdx.x] = g.mean[id];
-        s_con[threadIdx.x] = g.conic[id];
+        s_con[threadIdx.x] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.f);
         s_w[threadIdx.x] = __ldg(weight + id);
       }
       __syncthreads();
-      const int nb = min(NPIX, total - b0);
-      if (inside) {
-        for (int k = 0; k < nb; ++k) {
-          const float2 m = s_mean[k];
-          const float dx = m.x - pxf, dy = m.y - pyf;
-          const float4 con = s_con[k];
-          const float power = -0.5f * (con.x * dx * dx + con.z * dy * dy) - con.y * dx * dy;
-          if (power > 0.f) continue;
-          const float G = expf(power);
-          if (G < 1e-7f) continue;
-          const float2 wk = s_w[k];
-          c0 += wk.x * G;
-          c1 += wk.y * G;
+      const int nb = min(NTR, total - c0);
+      for (int k = 0; k < nb; ++k) {
+        const float2 m = s_mean[k];
+        const float4 con = s_con[k];
+        const float2 wk = s_w[k];
+        const float dx = m.x - pxf;
+        const float p0 = -con.x * dx * dx, h = con.y * dx;
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+          const float G = gauss_term(p0, h, con.z, m.y - pyf[r]);
+          acc_re[r] = fmaf(wk.x, G, acc_re[r]);
+          acc_im[r] = fmaf(wk.y, G, acc_im[r]);
         }
       }
       __syncthreads();
     }
   }
-  if (inside) {
-    out[size_t(py) * W + px] = c0;
-    out[size_t(H) * W + size_t(py) * W + px] = c1;
+  const size_t plane = size_t(H) * W;
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) {
+    const int y = py + RSTEP * r;
+    if (px < W && y < H) {
+      out[size_t(y) * W + px] = acc_re[r];
+      out[plane + size_t(y) * W + px] = acc_im[r];
+    }
   }
 }
 
@@ -255,30 +285,34 @@ __global__ void __launch_bounds__(32 * WARPS_BWD) k_gs_bwd(const float* __restri
     const float2 w = __ldg(weight + i);
     const float* g0 = gout;
     const float* g1 = gout + size_t(H) * W;
+    const float czh = 0.5f * con.z;
+    const int lx = lane & (TILE - 1), ly = lane / TILE;  // lane -> pixel (lx, ly + 2k) of each tile
     for (int ty = rc.y; ty < rc.w; ++ty)
-      for (int tx = rc.x; tx < rc.z; ++tx)
-#pragma unroll 4
+      for (int tx = rc.x; tx < rc.z; ++tx) {
+        const int px = tx * TILE + lx;
+        const float dx = m.x - float(px);
+        const float p0 = -0.5f * con.x * dx * dx, h = con.y * dx;
+        const float mxc = -con.x * dx, myc = -con.y * dx, c0c = -0.5f * dx * dx;
+#pragma unroll
         for (int k = 0; k < NPIX / 32; ++k) {
-          const int p = lane + 32 * k;
-          const int px = tx * TILE + (p & (TILE - 1)), py = ty * TILE + p / TILE;
-          if (px >= W || py >= H) continue;
-          const float dx = m.x - float(px), dy = m.y - float(py);
-          const float power = -0.5f * (con.x * dx * dx + con.z * dy * dy) - con.y * dx * dy;
-          if (power > 0.f) continue;
-          const float G = expf(power);
-          if (G < 1e-7f) continue;
+          const int py = ty * TILE + ly + 2 * k;
+          const float dy = m.y - float(py);
+          float G = gauss_term(p0, h, czh, dy);
+          const bool ok = G != 0.f && px < W && py < H;  // terms that are zero add nothing
+          G = ok ? G : 0.f;
           const size_t q = size_t(py) * W + px;
-          const float d0 = __ldg(g0 + q), d1 = __ldg(g1 + q);
-          const float dLdG = w.x * d0 + w.y * d1;
-          gw0 += G * d0;
-          gw1 += G * d1;
-          gmx += dLdG * (G * (-con.x * dx - con.y * dy));
-          gmy += dLdG * (G * (-con.z * dy - con.y * dx));
-          const float gdx = G * dx, gdy = G * dy;
-          gc0 += -0.5f * gdx * dx * dLdG;
-          gc1 += -gdx * dy * dLdG;
-          gc2 += -0.5f * gdy * dy * dLdG;
+          const float d0 = ok ? __ldg(g0 + q) : 0.f, d1 = ok ? __ldg(g1 + q) : 0.f;
+          const float u = G * fmaf(w.y, d1, w.x * d0);  // G dL/dG
+          gw0 = fmaf(G, d0, gw0);
+          gw1 = fmaf(G, d1, gw1);
+          gmx = fmaf(u, fmaf(-con.y, dy, mxc), gmx);  // dG/ddx = G (-cx dx - cy dy)
+          gmy = fmaf(u, fmaf(-con.z, dy, myc), gmy);  // dG/ddy = G (-cz dy - cy dx)
+          const float v = u * dy;
+          gc0 = fmaf(u, c0c, gc0);         // -0.5 G dx^2 dL/dG
+          gc1 = fmaf(-dx, v, gc1);         // -G dx dy dL/dG
+          gc2 = fmaf(-0.5f * dy, v, gc2);  // -0.5 G dy^2 dL/dG
         }
+      }
   }
   gw0 = warp_sum_f(gw0);
   gw1 = warp_sum_f(gw1);
@@ -382,7 +416,7 @@ int ptycho_gs_forward(int kind, const float* xy, const float* p1, const float* p
   else
     gs::k_gs_pre<PTYCHO_GS_CHOLESKY><<<nb, 256, 0, s>>>(xy, p1, p2, N, H, W, L.tx, L.ty, L.NW, L.NV, mxs, min_scale,
                                                         g, radii_out);
-  gs::k_gs_render<<<unsigned(T), gs::NPIX, 0, s>>>(reinterpret_cast<const float2*>(weight), H, W, L.tx, L.NW, L.NV,
+  gs::k_gs_render<<<unsigned(T), gs::NTR, 0, s>>>(reinterpret_cast<const float2*>(weight), H, W, L.tx, L.NW, L.NV,
                                                    g, out);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
