@@ -610,12 +610,44 @@ def run_gs(args):
     leaves = [torch.from_numpy(a).to(dev).requires_grad_(True) for a in (xy, p1, p2, wt)]
     fn = pkg.gsplat.GaussianRasterize2DCholesky
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    impl = "ours"
 
     def step():
         for t in leaves:
             t.grad = None
         out = fn.apply(*leaves, H, W, 16, 0.5)
         out.backward(gout)
+
+    if args.impl == "reference":
+        # the reference's own rasteriser (gscp/csrc/gscp_rasterizer, compiled from
+        # its sources with its flags into oracle/_ref), same scene, same GPU
+        import ctypes
+        so = os.path.join(ROOT, "oracle", "_ref", "libgscp_ref.so")
+        if not os.path.exists(so):
+            print(json.dumps({"impl": "reference", "metric": "Gaussian-field render fwd+bwd",
+                              "unavailable": "oracle/_ref/libgscp_ref.so was not built (needs the reference tree)"}))
+            return
+        L = ctypes.CDLL(so)
+        vp, ci, cf = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        L.gscp_ref_create.restype = vp
+        L.gscp_ref_forward.argtypes = [vp, ci, ci, ci, ci, vp, vp, vp, vp, ci, cf, vp, vp]
+        L.gscp_ref_backward.argtypes = [vp, ci, ci, ci, ci, vp, vp, vp, vp, ci, cf, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.gscp_ref_destroy.argtypes = [vp]
+        xy_d, p1_d, p2_d, w_d = (t.detach() for t in leaves)
+        out = torch.empty((2, H, W), device=dev)
+        radii = torch.empty(N, dtype=torch.int32, device=dev)
+        bufs = [torch.empty(s, device=dev) for s in ((N, 2), (N, 3), (N, 2), (N, 2), (N, 2), (N,))]
+        h = L.gscp_ref_create()
+        impl = "reference"
+
+        def step():  # noqa: F811 -- the reference arm's step
+            for b in bufs:  # the reference accumulates its gradients with atomicAdd
+                b.zero_()
+            assert L.gscp_ref_forward(h, 1, N, H, W, xy_d.data_ptr(), p1_d.data_ptr(), p2_d.data_ptr(),
+                                      w_d.data_ptr(), 16, 0.5, out.data_ptr(), radii.data_ptr()) >= 0
+            assert L.gscp_ref_backward(h, 1, N, H, W, xy_d.data_ptr(), p1_d.data_ptr(), p2_d.data_ptr(),
+                                       w_d.data_ptr(), 16, 0.5, radii.data_ptr(), gout.data_ptr(),
+                                       *[b.data_ptr() for b in bufs]) == 0
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -636,7 +668,12 @@ def run_gs(args):
             "config": {"workload": f"{N} Cholesky Gaussians, 512^2 grid, sigma 0.6-3 px, 16x16 tiles",
                        "l2": "flushed before every timed step"},
             "gpu_launches_per_step": 5, "dtype": "f32", "data": "synthetic (seeded)"}
-    if not args.no_cpu_baseline:
+    if impl == "reference":
+        line.update({"impl": "reference", "gpu_launches_per_step": None,
+                     "note": "the reference's rasteriser compiled from its CUDA sources (-O3 --use_fast_math), "
+                             "with its host read-back of the tile-pair count and its radix sort"})
+        L.gscp_ref_destroy(h)
+    elif not args.no_cpu_baseline:
         from oracle import gsplat as og  # the CPU restatement, timed as the baseline only
         n = min(N, 40000)
         t0 = time.perf_counter()
