@@ -153,14 +153,35 @@ def cpu_reference_rate(work, batch: int, budget_s: float, threads: int | None = 
     rng = np.random.default_rng(5)
     n, t_total, steps = 0, 0.0, 0
     lt = work["workload"].loss_type
+    first = None
     while t_total < budget_s or steps == 0:
         idx = rng.permutation(F)[:batch]
         t0 = time.perf_counter()
-        torch_cpu_path.minibatch_fwd_adj(obj, probe, work["tlY"], work["tlX"], stack, idx, lt)
+        loss = torch_cpu_path.minibatch_fwd_adj(obj, probe, work["tlY"], work["tlX"], stack, idx, lt)
         t_total += time.perf_counter() - t0
+        if first is None:  # kept to check the GPU path on the same minibatch
+            first = {"idx": idx.copy(), "loss": loss, "dO": obj.grad.detach().clone(),
+                     "dP": probe.grad.detach().clone()}
         n += len(idx)
         steps += 1
-    return n / t_total, n, steps, torch.get_num_threads()
+    return n / t_total, n, steps, torch.get_num_threads(), first
+
+
+def parity_vs_cpu(pkg, work, first, dev):
+    """The GPU path on the CPU baseline's first minibatch: relative errors of
+    the loss, dO and dP against the reference restatement (torch CPU, complex64)."""
+    w = work["workload"]
+    idx = first["idx"].astype(np.int32)
+    O = torch.from_numpy(work["obj"].astype(np.complex64)).to(dev)
+    P = torch.from_numpy(work["probe"].astype(np.complex64)).to(dev)
+    tl = pkg.make_windows(work["tlY"], work["tlX"], dev)
+    stack = torch.from_numpy(work["Imeas"]).to(dev)
+    loss, _, dO, dP = pkg.fwd_adj_raw(O, P, tl, stack, pkg.LOSS_CODES[w.loss_type],
+                                      batch=torch.from_numpy(idx).to(dev))
+    rel = lambda a, b: float((a - b).abs().max() / b.abs().max())  # noqa: E731
+    return {"loss_rel_err": abs(float(loss) - first["loss"]) / abs(first["loss"]),
+            "dO_rel_err": rel(dO.cpu(), first["dO"]), "dP_rel_err": rel(dP.cpu(), first["dP"]),
+            "note": "max |GPU - CPU| / max |CPU| on the first sampled minibatch; both complex64"}
 
 
 def run_reference(args):
@@ -398,11 +419,12 @@ def run_ours(args):
                 "e2e_resident_stack": e2e_resident, "gpu_launches": launches,
                 "clocks": clk.summary()}
         if not args.no_cpu_baseline and world == 1:
-            rate, n, steps, cores = cpu_reference_rate(work, B, budget_s=args.cpu_budget)
+            rate, n, steps, cores, first = cpu_reference_rate(work, B, budget_s=args.cpu_budget)
             line["cpu_baseline"] = {"value": rate, "unit": "patterns/s", "cores": cores, "kind": "port",
                                     "sample": f"{steps} minibatches x {B} patterns ({n} patterns) of the "
                                               f"same workload, per-frame torch CPU loop + autograd "
-                                              f"(reference restatement), {cores} threads"}
+                                              f"(reference restatement), {cores} threads",
+                                    "parity_first_minibatch": parity_vs_cpu(pkg, work, first, dev)}
         if world == 1 and not args.no_ttr and args.workload == "c1":
             # the headline's second half: time-to-residual, INR vs pixel grid (c2)
             try:
