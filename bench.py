@@ -707,6 +707,59 @@ def run_gs(args):
     print(json.dumps(line), flush=True)
 
 
+def run_aux(args):
+    """The auxiliary kernels around the two hot loops, each timed alone with CUDA
+    events over --steps launches (L2 warm: they run between the hot kernels):
+    Haar sparsity and its backward (1024^2 object), the FP64 object error
+    (1024^2), probe centring/normalisation and its backward (128^2), and the
+    hash-encoder CSR build (262,144 coordinates, 16 levels, log2 T 18)."""
+    dev = torch.device("cuda")
+    pkg = importlib.import_module(PKG)
+    rng = np.random.default_rng(0)
+    c = lambda *s: torch.from_numpy((rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype(np.complex64)).to(dev)  # noqa: E731
+    obj, gt, probe = c(1024, 1024), c(1024, 1024), c(128, 128)
+    s = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(args.steps):
+            fn()
+        b.record(s)
+        torch.cuda.synchronize()
+        return 1e3 * a.elapsed_time(b) / args.steps  # us
+
+    ops = {}
+    leaf = obj.clone().requires_grad_(True)
+
+    def haar():
+        leaf.grad = None
+        pkg.probe_prep.haar_sparsity(leaf).backward()
+    ops["haar_sparsity fwd+bwd (1024^2)"] = (timed(haar), 1024 * 1024 * 8 * 3)
+    ops["object_error (1024^2, FP64)"] = (timed(lambda: pkg.accuracy.object_error(obj, gt)), 1024 * 1024 * 16)
+    pl = probe.clone().requires_grad_(True)
+    gp = c(128, 128)
+
+    def prep():
+        pl.grad = None
+        pkg.probe_prep.center_and_normalize_probe(pl).backward(gp)
+    ops["probe centre+normalise fwd+bwd (128^2)"] = (timed(prep), 128 * 128 * 8 * 5)
+    enc = pkg.hashgrid.Encoding(2, {"otype": "HashGrid", "n_levels": 16, "n_features_per_level": 2,
+                                    "log2_hashmap_size": 18, "base_resolution": 16,
+                                    "per_level_scale": float(np.exp(np.log(32) / 15))}).to(dev)
+    yy, xx = torch.meshgrid(torch.linspace(0, 1, 512, device=dev), torch.linspace(0, 1, 512, device=dev),
+                            indexing="ij")
+    coords = torch.stack([xx.flatten(), yy.flatten()], 1).contiguous()
+    ops["hash CSR build (262,144 coords, one-time)"] = (
+        timed(lambda: pkg.hashgrid._CSR(coords, enc.cfg, enc.n_entries)), 262144 * 16 * 4 * 12)
+    out = {k: {"us": round(v, 2), "GB/s_algorithmic": round(b / (v * 1e-6) / 1e9, 1)} for k, (v, b) in ops.items()}
+    print(json.dumps({"metric": "auxiliary kernels", "steps": args.steps, "ops": out,
+                      "note": "each op through its public Python call; inputs resident, L2 warm"}), flush=True)
+
+
 WORKLOADS_DESC = {"c2": "c2: 1024^2 canvas, 128^2 probe, 28x28 raster (784 frames), smooth_L1, batch 10; INR "
                         "16 levels x 2, log2 T 18, base 16, finest 512, 512^2 object grid (ds 2), MLP 64x2, "
                         "omega 10/1, probe initProbe + residual"}
@@ -730,6 +783,7 @@ def main():
     ap.add_argument("--ref-cap-s", type=float, default=90.0)
     ap.add_argument("--no-ttr", action="store_true", help="omit the time-to-residual object from the bench line")
     ap.add_argument("--gs", action="store_true", help="time the Gaussian-field rasteriser instead")
+    ap.add_argument("--aux", action="store_true", help="time the auxiliary kernels instead")
     ap.add_argument("--gs-gaussians", type=int, default=100000)
     args = ap.parse_args()
     if args.time_to_residual:
@@ -740,6 +794,9 @@ def main():
         return
     if args.gs:
         run_gs(args)
+        return
+    if args.aux:
+        run_aux(args)
         return
     if args.warmup < 3:
         args.warmup = 3

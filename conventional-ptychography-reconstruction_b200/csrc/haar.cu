@@ -21,7 +21,7 @@
 namespace pty {
 namespace hr {
 
-constexpr int NT = 256, PER = 4, MAXG = 1184;
+constexpr int NT = 256, PER = 1, MAXG = 1184;  // one 2x2 block per thread: enough warps to cover latency
 
 PTY_DEVI float sgnf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
 
@@ -134,7 +134,7 @@ int ptycho_haar_sparsity_backward(const float* img, int H, int W, const double* 
 namespace pty {
 namespace oe {
 
-constexpr int NT = 256, MAXG = 592;
+constexpr int NT = 256, MAXG = 1184;
 
 __global__ void __launch_bounds__(NT) k_obj_err_part(const float2* __restrict__ R, const float2* __restrict__ T,
                                                      int W, int y0, int y1, int x0, int x1,
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(32) k_obj_err_final(const double* __restrict__
 }
 
 inline int grid_for(long long n) {
-  const long long g = (n + NT * 8 - 1) / (NT * 8);
+  const long long g = (n + NT * 2 - 1) / (NT * 2);
   return g < 1 ? 1 : (g > MAXG ? MAXG : int(g));
 }
 

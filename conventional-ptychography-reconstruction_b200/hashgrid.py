@@ -127,9 +127,6 @@ class Encoding(torch.nn.Module):
         csr = _CSR(coords, self.cfg, self.n_entries)
         self._csr = self._csr[-3:] + [(key, coords, coords._version, csr)]
         return csr
-        csr = _CSR(coords, self.cfg, self.n_entries)
-        self._csr = self._csr[-3:] + [(coords, coords._version, csr)]
-        return csr
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:
         if not x.is_cuda:
