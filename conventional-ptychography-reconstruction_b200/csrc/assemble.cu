@@ -184,14 +184,107 @@ __global__ void __launch_bounds__(kPixBlock, 6) k_dP_terms(float2* __restrict__ 
   if (p == 0 && g == 0 && loss_total) loss_sum_block(loss_pat, B, loss_total);
 }
 
+// k_dP_terms with two adjacent probe pixels per thread: E', G and the partials
+// move as 16-byte loads and stores and each pattern's window corner is read
+// once per pair.  Same terms, same order, bitwise the same results (P must be
+// 16-byte aligned; the launcher falls back to k_dP_terms otherwise).
+__global__ void __launch_bounds__(kPixBlock, 4) k_dP_terms2(float2* __restrict__ Eb, const float2* __restrict__ O,
+                                                         const float2* __restrict__ P, const int2* __restrict__ tlb,
+                                                         int B, int W, int M, float2* __restrict__ part,
+                                                         unsigned* __restrict__ done, float2* __restrict__ dP,
+                                                         int want_G, int accumulate,
+                                                         const double* __restrict__ loss_pat,
+                                                         double* __restrict__ loss_total) {
+  __shared__ int last;
+  const int p = blockIdx.x, g = blockIdx.y, G = gridDim.y;
+  const int idx = 2 * (p * kPixBlock + threadIdx.x);  // even: the pair (x, x + 1) shares a row
+  const bool in = idx < M * M;
+  const int y = idx / M, x = idx - (idx / M) * M;
+  const bool want_dP = dP != nullptr;
+  const size_t MM = size_t(M) * M;
+  if (in) {
+    const int odd = (x + y) & 1;
+    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (want_G) pc = __ldg(reinterpret_cast<const float4*>(P + idx));
+    float2 acc0 = make_float2(0.f, 0.f), acc1 = make_float2(0.f, 0.f);
+    const int b1 = min(B, (g + 1) * kGroup);
+    constexpr int U = 4;  // patterns whose loads are in flight together
+    for (int b = g * kGroup; b < b1; b += U) {
+      float4 e[U];
+      float2 t0[U], t1[U];
+      bool ok[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const int2 c = b + k < b1 ? __ldg(tlb + b + k) : make_int2(-1, -1);
+        ok[k] = c.x >= 0;
+        e[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        t0[k] = t1[k] = make_float2(0.f, 0.f);
+        if (ok[k]) {
+          e[k] = __ldcg(reinterpret_cast<const float4*>(Eb + size_t(b + k) * MM + idx));
+          if (want_dP) {
+            const float2* o = O + size_t(c.x + y) * W + c.y + x;
+            t0[k] = c_mulc(make_float2(e[k].x, e[k].y), __ldg(o));
+            t1[k] = c_mulc(make_float2(e[k].z, e[k].w), __ldg(o + 1));
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        acc0 = c_add(acc0, t0[k]);  // ascending pattern order
+        acc1 = c_add(acc1, t1[k]);
+        if (want_G && ok[k]) {
+          const float2 g0 = c_negif(c_mulc(make_float2(e[k].x, e[k].y), make_float2(pc.x, pc.y)), odd);
+          const float2 g1 = c_negif(c_mulc(make_float2(e[k].z, e[k].w), make_float2(pc.z, pc.w)), odd ^ 1);
+          __stcg(reinterpret_cast<float4*>(Eb + size_t(b + k) * MM + idx), make_float4(g0.x, g0.y, g1.x, g1.y));
+        }
+      }
+    }
+    if (want_dP) {
+      const float2 a0 = c_negif(acc0, odd), a1 = c_negif(acc1, odd ^ 1);
+      __stcg(reinterpret_cast<float4*>(part + size_t(g) * MM + idx), make_float4(a0.x, a0.y, a1.x, a1.y));
+    }
+  }
+  if (want_dP) {  // uniform over the grid
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(done + p, 1u) == unsigned(G - 1));
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      if (in) {
+        float2 r0 = make_float2(0.f, 0.f), r1 = make_float2(0.f, 0.f);
+        for (int gg = 0; gg < G; ++gg) {
+          const float4 v = __ldcg(reinterpret_cast<const float4*>(part + size_t(gg) * MM + idx));
+          r0 = c_add(r0, make_float2(v.x, v.y));
+          r1 = c_add(r1, make_float2(v.z, v.w));
+        }
+        if (accumulate) {
+          r0 = c_add(dP[idx], r0);
+          r1 = c_add(dP[idx + 1], r1);
+        }
+        dP[idx] = r0;
+        dP[idx + 1] = r1;
+      }
+      if (threadIdx.x == 0) done[p] = 0u;  // ready for the next call
+    }
+  }
+  if (p == 0 && g == 0 && loss_total) loss_sum_block(loss_pat, B, loss_total);
+}
+
 int launch_assemble(float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W, int M,
                     float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
                     double* loss_total, bool accumulate, cudaStream_t s) {
   if (dO || dP) {  // dP partials and, for dO, the in-place E' -> G conversion
     const int G = (B + kGroup - 1) / kGroup;
-    dim3 grid(dp_counters(M), G);
-    k_dP_terms<<<grid, kPixBlock, 0, s>>>(Eb, O, P, tlb, B, W, M, part, done, dP, dO ? 1 : 0, accumulate ? 1 : 0,
-                                          loss_pat, loss_total);
+    if ((reinterpret_cast<uintptr_t>(P) & 15) == 0) {  // pairs of pixels, 16-byte accesses
+      dim3 grid((M * M / 2 + kPixBlock - 1) / kPixBlock, G);
+      k_dP_terms2<<<grid, kPixBlock, 0, s>>>(Eb, O, P, tlb, B, W, M, part, done, dP, dO ? 1 : 0,
+                                             accumulate ? 1 : 0, loss_pat, loss_total);
+    } else {
+      dim3 grid(dp_counters(M), G);
+      k_dP_terms<<<grid, kPixBlock, 0, s>>>(Eb, O, P, tlb, B, W, M, part, done, dP, dO ? 1 : 0,
+                                            accumulate ? 1 : 0, loss_pat, loss_total);
+    }
   } else if (loss_total) {
     k_loss_total<<<1, 256, 0, s>>>(loss_pat, B, loss_total);
   }

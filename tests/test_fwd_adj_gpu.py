@@ -198,6 +198,28 @@ def test_deterministic_bitwise(pkg):
     assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
 
 
+@pytest.mark.parametrize("M", [64, 128])
+def test_probe_alignment_paths_agree_bitwise(pkg, M):
+    """A probe that is 8- but not 16-byte aligned takes the one-pixel-per-thread
+    dP assembly; a 16-byte aligned one the paired kernel.  Same results, bitwise."""
+    O, P, tlY, tlX, Imeas = _case(M, 2 * M + 40, 37, seed=9)
+    dev = torch.device("cuda")
+    Ot = torch.from_numpy(O).to(dev)
+    tl = pkg.make_windows(tlY, tlX, dev)
+    Im = torch.from_numpy(Imeas).to(dev)
+    buf = torch.zeros(M * M + 1, dtype=torch.complex64, device=dev)
+    P_odd = buf[1:].view(M, M)  # starts 8 bytes into an aligned allocation
+    P_odd.copy_(torch.from_numpy(P))
+    P_al = torch.from_numpy(P).to(dev)
+    assert P_odd.data_ptr() % 16 == 8 and P_al.data_ptr() % 16 == 0
+    res = []
+    for Pt in (P_al, P_odd):
+        loss, _, dO, dP = pkg.fwd_adj_raw(Ot, Pt, tl, Im, pkg.LOSS_CODES["Poisson_likelihood_loss"])
+        res.append((float(loss), dO.cpu(), dP.cpu()))
+    assert res[0][0] == res[1][0]
+    assert torch.equal(res[0][1], res[1][1]) and torch.equal(res[0][2], res[1][2])
+
+
 def test_edge_windows_and_uncovered_canvas(pkg):
     """Windows touching all four canvas edges; a region no window covers gets exactly 0."""
     M = 64
