@@ -409,7 +409,7 @@ def run_ours(args):
         achieved = bpp * B / step_s / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": f"of {kind}",
-                "kernel": "ptycho_fwd_adj (k_fused + k_dP_terms + k_dO), one CUDA-graph launch per minibatch",
+                "kernel": "ptycho_fwd_adj (k_fused + k_dP_terms2 + k_dO), one CUDA-graph launch per minibatch",
                 "algorithmic_bytes_per_pattern": bpp, "traffic": load_traffic(f"{args.workload}_fwd_adj")}
         line = {"metric": METRIC, "value": value, "unit": "patterns/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps, "higher_is_better": True,
