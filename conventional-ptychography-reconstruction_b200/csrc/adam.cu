@@ -144,3 +144,54 @@ extern "C" int ptycho_adam_step(float* const* params, const float* const* grads,
                                                                    (float)(1.0 / sqrt(bc2)), eps);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
+
+// ---- chain rule through the fused loss: scaled copies of dO and dP --------
+// The fused forward/adjoint produces dL/dO and dL/dP for a unit upstream
+// gradient; autograd's backward multiplies both by the upstream scalar g
+// (a device float).  One grid-stride launch covers both arrays (float4 where
+// both pointers are 16-byte aligned), out of place so the saved gradients stay
+// valid for a second backward.
+namespace pty {
+namespace gsc {
+
+__global__ void __launch_bounds__(256) k_scale_pair(const float* __restrict__ a, float* __restrict__ ao, long long na,
+                                                    const float* __restrict__ b, float* __restrict__ bo, long long nb,
+                                                    const float* __restrict__ g, int vec_a, int vec_b) {
+  const float s = __ldg(g);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long qa = vec_a ? na / 4 : 0, qb = vec_b ? nb / 4 : 0;
+  for (long long i = t0; i < qa; i += stride) {
+    float4 v = __ldg(reinterpret_cast<const float4*>(a) + i);
+    reinterpret_cast<float4*>(ao)[i] = make_float4(v.x * s, v.y * s, v.z * s, v.w * s);
+  }
+  for (long long i = 4 * qa + t0; i < na; i += stride) ao[i] = a[i] * s;
+  for (long long i = t0; i < qb; i += stride) {
+    float4 v = __ldg(reinterpret_cast<const float4*>(b) + i);
+    reinterpret_cast<float4*>(bo)[i] = make_float4(v.x * s, v.y * s, v.z * s, v.w * s);
+  }
+  for (long long i = 4 * qb + t0; i < nb; i += stride) bo[i] = b[i] * s;
+}
+
+}  // namespace gsc
+}  // namespace pty
+
+extern "C" int ptycho_scale_pair(const float* a, float* a_out, long long na, const float* b, float* b_out,
+                                 long long nb, const float* scale, ptycho_stream_t stream) {
+  if (!scale || na < 0 || nb < 0 || (na > 0 && (!a || !a_out)) || (nb > 0 && (!b || !b_out)))
+    return PTYCHO_ERR_INVALID_ARG;
+  if (!pty_aligned(a, 4) || !pty_aligned(a_out, 4) || !pty_aligned(b, 4) || !pty_aligned(b_out, 4) ||
+      !pty_aligned(scale, 4))
+    return PTYCHO_ERR_MISALIGNED;
+  if (na + nb == 0) return PTYCHO_OK;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long work = (na + nb) / 4 + 1;
+  const long long want = (work + 255) / 256;
+  const int grid = int(want < 8LL * nsm ? want : 8LL * nsm);
+  const int va = pty_aligned(a, 16) && pty_aligned(a_out, 16), vb = pty_aligned(b, 16) && pty_aligned(b_out, 16);
+  pty::gsc::k_scale_pair<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a, a_out, na, b, b_out, nb,
+                                                                                    scale, va, vb);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}

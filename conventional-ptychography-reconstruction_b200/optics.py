@@ -300,13 +300,16 @@ class _FusedLoss(torch.autograd.Function):
         if not ctx.need:
             return None, None, None, None, None, None
         dO, dP = ctx.saved_tensors
-        s = g.to(torch.float32)
-        want = [t for t, n in ((dO, ctx.needs_input_grad[0]), (dP, ctx.needs_input_grad[1])) if n]
-        # one multi-tensor launch scales both gradients (real views, out of place)
-        scaled = iter(torch.view_as_complex(t) for t in
-                      torch._foreach_mul([torch.view_as_real(t) for t in want], s))
-        gO = next(scaled) if ctx.needs_input_grad[0] else None
-        gP = next(scaled) if ctx.needs_input_grad[1] else None
+        s = g.to(torch.float32).contiguous()
+        gO = torch.empty_like(dO) if ctx.needs_input_grad[0] else None
+        gP = torch.empty_like(dP) if ctx.needs_input_grad[1] else None
+        # one launch scales both gradients by the upstream scalar (out of place:
+        # the saved dO/dP stay valid for a second backward)
+        ptr = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+        _lib.check(_lib.lib().ptycho_scale_pair(
+            ptr(dO if gO is not None else None), ptr(gO), 2 * dO.numel() if gO is not None else 0,
+            ptr(dP if gP is not None else None), ptr(gP), 2 * dP.numel() if gP is not None else 0,
+            s.data_ptr(), torch.cuda.current_stream(s.device).cuda_stream), "ptycho_scale_pair")
         return gO, gP, None, None, None, None
 
 

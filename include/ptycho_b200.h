@@ -235,6 +235,16 @@ int ptycho_adam_step_dev(float* const* params, const float* const* grads, float*
                          ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Chain rule through the fused loss: a_out = g * a (na floats) and
+ * b_out = g * b (nb floats) in one launch, g = *scale a device float (the
+ * upstream gradient autograd hands the fused loss's backward).  Used for dO
+ * and dP (complex64 as their float views).  No counterpart in the reference,
+ * where autograd scales each gradient inside its own backward graph.
+ * ---------------------------------------------------------------------- */
+int ptycho_scale_pair(const float* a, float* a_out, long long na, const float* b, float* b_out,
+                      long long nb, const float* scale, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * Fourier upsampling of the INR object.  Replaces fourier_upsample of
  * models/complex_inr.py:252-271 (called at :287):
  *   y = ifft2(ifftshift(pad(fftshift(fft2(x))))) * s^2,

@@ -121,6 +121,15 @@ def test_gsplat_validation_before_device_work():
                                 fake, fake, fake, fake, None) == 1
 
 
+def test_scale_pair_validation_before_device_work():
+    L = load_pkg().lib()
+    fake = ctypes.c_void_p(4096)
+    assert L.ptycho_scale_pair(fake, fake, 8, fake, fake, 8, None, None) == 1  # no scale
+    assert L.ptycho_scale_pair(None, fake, 8, fake, fake, 8, fake, None) == 1
+    assert L.ptycho_scale_pair(ctypes.c_void_p(4098), fake, 8, fake, fake, 8, fake, None) == 3
+    assert L.ptycho_scale_pair(None, None, 0, None, None, 0, fake, None) == 0  # nothing to do
+
+
 def test_workspace_size_monotone():
     L = load_pkg().lib()
     a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)

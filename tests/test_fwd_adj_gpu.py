@@ -292,6 +292,21 @@ def test_fused_loss_autograd(pkg):
     assert rel_max(Pt.grad.cpu().numpy(), 3 * r["dP"]) <= 2e-4
 
 
+def test_fused_loss_backward_one_input_twice(pkg):
+    """Only the object needs a gradient; a retained graph backs up twice and the
+    scaled copies leave the saved gradients intact (accumulates 2 x 0.5 dO)."""
+    dev = torch.device("cuda")
+    O, P, tlY, tlX, Imeas = _case(64, 120, 5, seed=17)
+    Ot = torch.from_numpy(O).to(dev).requires_grad_(True)
+    Pt = torch.from_numpy(P).to(dev)
+    loss = pkg.fused_loss(Ot, Pt, pkg.make_windows(tlY, tlX, dev), torch.from_numpy(Imeas).to(dev),
+                          "Poisson_likelihood_loss")
+    (0.5 * loss).backward(retain_graph=True)
+    (0.5 * loss).backward()
+    r = fm.fwd_adj(O, P, tlY, tlX, Imeas, "Poisson_likelihood_loss")
+    assert rel_max(Ot.grad.cpu().numpy(), r["dO"]) <= 2e-4
+
+
 def test_frame_id_batches(pkg):
     """Frame ids select rows of a resident stack (Recovery.py's perm slice)."""
     dev = torch.device("cuda")
