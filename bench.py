@@ -179,9 +179,18 @@ def parity_vs_cpu(pkg, work, first, dev):
     loss, _, dO, dP = pkg.fwd_adj_raw(O, P, tl, stack, pkg.LOSS_CODES[w.loss_type],
                                       batch=torch.from_numpy(idx).to(dev))
     rel = lambda a, b: float((a - b).abs().max() / b.abs().max())  # noqa: E731
-    return {"loss_rel_err": abs(float(loss) - first["loss"]) / abs(first["loss"]),
-            "dO_rel_err": rel(dO.cpu(), first["dO"]), "dP_rel_err": rel(dP.cpu(), first["dP"]),
-            "note": "max |GPU - CPU| / max |CPU| on the first sampled minibatch; both complex64"}
+    out = {"vs_torch_cpu_complex64": {
+        "loss_rel_err": abs(float(loss) - first["loss"]) / abs(first["loss"]),
+        "dO_rel_err": rel(dO.cpu(), first["dO"]), "dP_rel_err": rel(dP.cpu(), first["dP"])}}
+    from oracle import forward_model as fm  # the FP64 NumPy oracle, as the checker
+    ref = fm.fwd_adj(work["obj"], work["probe"], work["tlY"][idx], work["tlX"][idx], work["Imeas"][idx],
+                     w.loss_type)
+    rn = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())  # noqa: E731
+    out["vs_fp64_oracle"] = {"loss_rel_err": abs(float(loss) - ref["loss_total"]) / abs(ref["loss_total"]),
+                             "dO_rel_err": rn(dO.cpu().numpy(), ref["dO"]),
+                             "dP_rel_err": rn(dP.cpu().numpy(), ref["dP"])}
+    out["note"] = "max |GPU - ref| / max |ref| on the CPU baseline's first sampled minibatch"
+    return out
 
 
 def run_reference(args):
@@ -699,11 +708,20 @@ def run_gs(args):
         from oracle import gsplat as og  # the CPU restatement, timed as the baseline only
         n = min(N, 40000)
         t0 = time.perf_counter()
-        og.render(og.CHOLESKY, xy[:n], p1[:n], p2[:n], wt[:n], H, W, 16, 0.5)
-        og.backward(og.CHOLESKY, xy[:n], p1[:n], p2[:n], wt[:n], H, W, 16, 0.5, gout.cpu().numpy())
+        ref_img, _ = og.render(og.CHOLESKY, xy[:n], p1[:n], p2[:n], wt[:n], H, W, 16, 0.5)
+        ref_g = og.backward(og.CHOLESKY, xy[:n], p1[:n], p2[:n], wt[:n], H, W, 16, 0.5, gout.cpu().numpy())
         dt = time.perf_counter() - t0
+        # the kernels on the same subset, checked against that float64 restatement
+        sub = [t.detach()[:n].clone().requires_grad_(True) for t in leaves]
+        img = fn.apply(*sub, H, W, 16, 0.5)
+        img.backward(gout)
+        rn = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))  # noqa: E731
+        parity = {"image_rel_err": rn(img.detach().cpu().numpy(), ref_img)}
+        for name, t, r in zip(("dxy", "dlog_L_diag", "dL_offdiag", "dweight"), sub, ref_g):
+            parity[name + "_rel_err"] = rn(t.grad.cpu().numpy().reshape(r.shape), r)
         line["cpu_baseline"] = {"value": n / dt, "unit": "Gaussians/s", "cores": 1, "kind": "port",
-                                "sample": f"first {n} Gaussians of the same scene, NumPy restatement, fwd+bwd"}
+                                "sample": f"first {n} Gaussians of the same scene, NumPy restatement, fwd+bwd",
+                                "parity_vs_oracle": parity}
     print(json.dumps(line), flush=True)
 
 
