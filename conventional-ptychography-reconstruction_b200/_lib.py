@@ -44,6 +44,9 @@ SIGNATURES = {
     "ptycho_gs_backward": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp,
                                     _c_size, _vp, _vp, _vp, _vp, _vp]),
     "ptycho_scale_pair": (_c_int, [_vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _vp]),
+    "ptycho_residual_workspace_size": (_c_size, []),
+    "ptycho_residual": (_c_int, [_vp, _vp, _vp, _c_ll, _vp, _vp]),
+    "ptycho_residual_backward": (_c_int, [_vp, _vp, _vp, _c_ll, _vp, _vp, _vp, _c_size, _vp]),
     "ptycho_hashgrid_entries": (_c_int, [_c_int, _c_int, _c_int, _c_float]),
     "ptycho_hashgrid_forward": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),
     "ptycho_hashgrid_forward_planar": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_float, _vp, _vp]),

@@ -15,9 +15,40 @@ import torch
 import torch.nn as nn
 import torch.nn.functional as F
 
-from . import resample
+from . import _lib, resample
 from .cmlp import ComplexMLP
 from .hashgrid import Encoding
+
+
+class _Residual(torch.autograd.Function):
+    """out = k * m + init on the device (``ptycho_residual``), k a real 0-d
+    parameter; the backward gives k * g and sum Re(conj(g) m) in one launch."""
+
+    @staticmethod
+    def forward(ctx, k, m, init, ws):
+        mm = m.to(torch.complex64).contiguous()
+        ii = init.to(device=mm.device, dtype=torch.complex64).contiguous()
+        kk = k.detach().to(torch.float32).contiguous()
+        out = torch.empty_like(mm)
+        _lib.check(_lib.lib().ptycho_residual(kk.data_ptr(), mm.data_ptr(), ii.data_ptr(), mm.numel(),
+                                              out.data_ptr(), torch.cuda.current_stream(mm.device).cuda_stream),
+                   "ptycho_residual")
+        ctx.save_for_backward(kk, mm)
+        ctx.ws, ctx.kshape = ws, k.shape
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        kk, mm = ctx.saved_tensors
+        gc = g.to(torch.complex64).contiguous()
+        gm = torch.empty_like(mm) if ctx.needs_input_grad[1] else None
+        gk = torch.empty((), dtype=torch.float32, device=mm.device)
+        _lib.check(_lib.lib().ptycho_residual_backward(
+            kk.data_ptr(), mm.data_ptr(), gc.data_ptr(), mm.numel(), gm.data_ptr() if gm is not None else None,
+            gk.data_ptr(), ctx.ws.data_ptr(), ctx.ws.numel(), torch.cuda.current_stream(mm.device).cuda_stream),
+            "ptycho_residual_backward")
+        return (gk.reshape(ctx.kshape) if ctx.needs_input_grad[0] else None, gm,
+                g if ctx.needs_input_grad[2] else None, None)
 
 
 class ComplexINRModel2D(nn.Module):
@@ -130,6 +161,14 @@ class ComplexINRModel2D(nn.Module):
         return model.net(coords)
 
     def apply_residual(self, complex_tensor, is_object=True):
-        if is_object:
-            return self.k_object * complex_tensor + self.object_initial if self.has_object_residual else complex_tensor
-        return self.k_probe * complex_tensor + self.probe_initial if self.has_probe_residual else complex_tensor
+        """k * network + initial (models/complex_inr.py:316-334) as one kernel
+        forward and one backward (``ptycho_residual``)."""
+        if is_object and not self.has_object_residual or not is_object and not self.has_probe_residual:
+            return complex_tensor
+        k, init = (self.k_object, self.object_initial) if is_object else (self.k_probe, self.probe_initial)
+        dev = complex_tensor.device
+        ws = getattr(self, "_residual_ws", None)
+        if ws is None or ws.device != dev:  # zeroed once; every backward leaves it zeroed
+            ws = torch.zeros(int(_lib.lib().ptycho_residual_workspace_size()), dtype=torch.uint8, device=dev)
+            self._residual_ws = ws
+        return _Residual.apply(k, complex_tensor, init, ws)

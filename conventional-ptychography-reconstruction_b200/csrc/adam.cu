@@ -195,3 +195,104 @@ extern "C" int ptycho_scale_pair(const float* a, float* a_out, long long na, con
                                                                                     scale, va, vb);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
+
+// ---- residual composition k * m + init (models/complex_inr.py:132-135) ----
+// k is a real float32 scalar in device memory, m and init complex64 [n].
+// Forward: out = k m + init.  Backward (torch's complex convention, k real):
+// gm = k g and gk = sum Re(conj(g) m), the sum in FP64 with fixed per-thread
+// ranges, a fixed tree per CTA and the CTA partials added in order by the
+// last-arriving CTA (integer counter, reset for the next call): one launch.
+namespace pty {
+namespace rsd {
+
+constexpr int NT = 256, MAXG = 592;
+
+__global__ void __launch_bounds__(NT) k_residual_fwd(const float* __restrict__ k, const float2* __restrict__ m,
+                                                     const float2* __restrict__ init, long long n,
+                                                     float2* __restrict__ out) {
+  const float kk = __ldg(k);
+  for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT) {
+    const float2 a = __ldg(m + i), b = __ldg(init + i);
+    out[i] = make_float2(fmaf(kk, a.x, b.x), fmaf(kk, a.y, b.y));
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_residual_bwd(const float* __restrict__ k, const float2* __restrict__ m,
+                                                     const float2* __restrict__ g, long long n,
+                                                     float2* __restrict__ gm, float* __restrict__ gk,
+                                                     double* __restrict__ part, unsigned* __restrict__ counter) {
+  __shared__ double red[NT / 32];
+  __shared__ bool last;
+  const float kk = __ldg(k);
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT) {
+    const float2 a = __ldg(m + i), d = __ldg(g + i);
+    if (gm) gm[i] = make_float2(kk * d.x, kk * d.y);
+    s += double(d.x) * a.x + double(d.y) * a.y;  // Re(conj(g) m)
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < NT / 32; ++w) t += red[w];
+    part[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+    double t = 0.0;
+    for (int b = threadIdx.x; b < int(gridDim.x); b += 32) t += __ldcg(part + b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) {
+      *gk = float(t);
+      *counter = 0u;  // ready for the next call
+    }
+  }
+}
+
+inline int grid_for(long long n) {
+  const long long g = (n + NT * 4 - 1) / (NT * 4);
+  return g < 1 ? 1 : (g > MAXG ? MAXG : int(g));
+}
+
+}  // namespace rsd
+}  // namespace pty
+
+extern "C" {
+
+size_t ptycho_residual_workspace_size(void) { return size_t(pty::rsd::MAXG) * sizeof(double) + 256; }
+
+int ptycho_residual(const float* k, const float* m, const float* init, long long n, float* out,
+                    ptycho_stream_t stream) {
+  if (!k || !m || !init || !out || n < 0) return PTYCHO_ERR_INVALID_ARG;
+  if (!pty_aligned(k, 4) || !pty_aligned(m, 8) || !pty_aligned(init, 8) || !pty_aligned(out, 8))
+    return PTYCHO_ERR_MISALIGNED;
+  if (n == 0) return PTYCHO_OK;
+  pty::rsd::k_residual_fwd<<<pty::rsd::grid_for(n), pty::rsd::NT, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      k, reinterpret_cast<const float2*>(m), reinterpret_cast<const float2*>(init), n,
+      reinterpret_cast<float2*>(out));
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+int ptycho_residual_backward(const float* k, const float* m, const float* g, long long n, float* gm, float* gk,
+                             void* workspace, size_t workspace_bytes, ptycho_stream_t stream) {
+  if (!k || !m || !g || !gk || n < 0) return PTYCHO_ERR_INVALID_ARG;
+  if (!workspace || workspace_bytes < ptycho_residual_workspace_size()) return PTYCHO_ERR_WORKSPACE;
+  if (!pty_aligned(k, 4) || !pty_aligned(m, 8) || !pty_aligned(g, 8) || !pty_aligned(gm, 8) ||
+      !pty_aligned(gk, 4) || !pty_aligned(workspace, 256))
+    return PTYCHO_ERR_MISALIGNED;
+  double* part = static_cast<double*>(workspace);
+  unsigned* counter = reinterpret_cast<unsigned*>(static_cast<char*>(workspace) +
+                                                  size_t(pty::rsd::MAXG) * sizeof(double));
+  pty::rsd::k_residual_bwd<<<pty::rsd::grid_for(n), pty::rsd::NT, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      k, reinterpret_cast<const float2*>(m), reinterpret_cast<const float2*>(g), n, reinterpret_cast<float2*>(gm),
+      gk, part, counter);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+}
+
+}  // extern "C"

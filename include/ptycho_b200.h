@@ -245,6 +245,24 @@ int ptycho_scale_pair(const float* a, float* a_out, long long na, const float* b
                       long long nb, const float* scale, ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Residual composition of the INR output, apply_residual of
+ * models/complex_inr.py:132-135: out = k * m + init, k a real float32 scalar
+ * in device memory, m / init / out complex64 [n].  The backward gives
+ * gm = k * g (skipped when gm is null) and *gk = sum Re(conj(g) m), summed in
+ * FP64 in a fixed order within one launch.  The workspace
+ * (ptycho_residual_workspace_size() bytes, 256-byte aligned) must be zeroed
+ * once before its first use; every call leaves it zeroed again.  Calls that
+ * share a workspace must not overlap on the GPU.
+ * ---------------------------------------------------------------------- */
+size_t ptycho_residual_workspace_size(void);
+
+int ptycho_residual(const float* k, const float* m, const float* init, long long n, float* out,
+                    ptycho_stream_t stream);
+
+int ptycho_residual_backward(const float* k, const float* m, const float* g, long long n, float* gm,
+                             float* gk, void* workspace, size_t workspace_bytes, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * Fourier upsampling of the INR object.  Replaces fourier_upsample of
  * models/complex_inr.py:252-271 (called at :287):
  *   y = ifft2(ifftshift(pad(fftshift(fft2(x))))) * s^2,

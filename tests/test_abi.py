@@ -130,6 +130,16 @@ def test_scale_pair_validation_before_device_work():
     assert L.ptycho_scale_pair(None, None, 0, None, None, 0, fake, None) == 0  # nothing to do
 
 
+def test_residual_validation_before_device_work():
+    L = load_pkg().lib()
+    fake = ctypes.c_void_p(4096)
+    n = L.ptycho_residual_workspace_size()
+    assert L.ptycho_residual(None, fake, fake, 8, fake, None) == 1
+    assert L.ptycho_residual(fake, ctypes.c_void_p(4100), fake, 8, fake, None) == 3
+    assert L.ptycho_residual_backward(fake, fake, fake, 8, fake, fake, fake, n - 8, None) == 4
+    assert L.ptycho_residual_backward(fake, fake, fake, 8, None, None, fake, n, None) == 1  # no gk
+
+
 def test_workspace_size_monotone():
     L = load_pkg().lib()
     a = L.ptycho_fwd_adj_workspace_size(1536, 1536, 128, 128, 256)
