@@ -479,6 +479,11 @@ def time_to_residual(args):
         return {"nrmse_phase": round(e["nrmse"], 5), "nrmse_scaled": round(e["nrmse_scaled"], 5)}
 
     def timed(trainer, max_epochs, max_s, target):
+        # garbage left by the previous arm (its CUDA graphs among it) is collected
+        # here, outside the timed epochs, not by the cyclic GC during them
+        import gc
+        gc.collect()
+        torch.cuda.synchronize()
         hist, t_train, reached = [], 0.0, None
         for ep in range(max_epochs):
             torch.cuda.synchronize()
