@@ -190,7 +190,23 @@ __global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ s
   if (e >= E) return;
   const int s0 = start[e], s1 = start[e + 1];
   float ax = 0.f, ay = 0.f;
-  for (int j = s0 + lane; j < s1; j += 32) {
+  int j = s0 + lane;
+  // four strides' loads in flight, then the adds in the same order as one at a time
+  for (; j + 96 < s1; j += 128) {
+    float w[4];
+    float2 g[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      w[k] = __ldg(weight + j + 32 * k);
+      g[k] = dfeat_at<PLANAR>(dfeat, __ldg(item + j + 32 * k), N);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ax = fmaf(w[k], g[k].x, ax);
+      ay = fmaf(w[k], g[k].y, ay);
+    }
+  }
+  for (; j < s1; j += 32) {
     const float w = __ldg(weight + j);
     const float2 g = dfeat_at<PLANAR>(dfeat, __ldg(item + j), N);
     ax = fmaf(w, g.x, ax);
@@ -221,7 +237,22 @@ __global__ void __launch_bounds__(256) k_hash_bwd_thread(const int* __restrict__
   if (e >= E) return;
   const int s0 = start[e], s1 = start[e + 1];
   float ax = 0.f, ay = 0.f;
-  for (int j = s0; j < s1; ++j) {
+  int j = s0;
+  for (; j + 3 < s1; j += 4) {  // four items' loads in flight, adds in order
+    float w[4];
+    float2 g[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      w[k] = __ldg(weight + j + k);
+      g[k] = dfeat_at<PLANAR>(dfeat, __ldg(item + j + k), N);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ax = fmaf(w[k], g[k].x, ax);
+      ay = fmaf(w[k], g[k].y, ay);
+    }
+  }
+  for (; j < s1; ++j) {
     const float w = __ldg(weight + j);
     const float2 g = dfeat_at<PLANAR>(dfeat, __ldg(item + j), N);
     ax = fmaf(w, g.x, ax);
