@@ -22,8 +22,21 @@ struct AdamList {
   float* m[kAdamMaxTensors];
   float* v[kAdamMaxTensors];
   long long end[kAdamMaxTensors];  // cumulative element counts
+  int blk_end[kAdamMaxTensors];    // cumulative block counts (chunked launch)
+  int vec[kAdamMaxTensors];        // p, g, m, v all 16-byte aligned
   int n;
 };
+
+constexpr int kAdamChunk = 256 * 4;  // elements per block of the chunked launch
+
+// one element of the update (the expressions of both launch forms)
+PTY_DEVI void adam_elem(float g, float& m, float& v, float& p, float lr_bc1, float b1, float b2,
+                        float inv_sqrt_bc2, float eps) {
+  m = fmaf(1.0f - b1, g - m, m);
+  v = fmaf(1.0f - b2, g * g, b2 * v);
+  const float denom = sqrtf(v) * inv_sqrt_bc2 + eps;
+  p -= lr_bc1 * (m / denom);
+}
 
 __global__ void __launch_bounds__(256) k_adam(const AdamList L, long long total, float lr_bc1, float b1, float b2,
                                               float inv_sqrt_bc2, float eps) {
@@ -47,8 +60,13 @@ __global__ void __launch_bounds__(256) k_adam(const AdamList L, long long total,
 // counter, every block derives the bias corrections from it
 __global__ void k_adam_tick(int* step) { step[0] += 1; }
 
-__global__ void __launch_bounds__(256) k_adam_dev(const AdamList L, long long total, const int* __restrict__ step,
-                                                  const float* __restrict__ lr, float b1, float b2, float eps) {
+// capturable step, chunked: block b owns elements [1024 c, 1024 c + 1024) of one
+// tensor (found once per block from the cumulative block counts), four per
+// thread with 16-byte accesses where the tensor allows; the per-element
+// arithmetic is adam_elem, so results equal the element-wise form bitwise.
+__global__ void __launch_bounds__(256) k_adam_dev_chunked(const AdamList L, const int* __restrict__ step,
+                                                          const float* __restrict__ lr, float b1, float b2,
+                                                          float eps) {
   __shared__ float sc[2];
   if (threadIdx.x == 0) {
     const double t = (double)step[0];
@@ -58,18 +76,38 @@ __global__ void __launch_bounds__(256) k_adam_dev(const AdamList L, long long to
   }
   __syncthreads();
   const float lr_bc1 = sc[0], inv_sqrt_bc2 = sc[1];
-  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < total; i += (long long)gridDim.x * 256) {
-    int k = 0;
-    while (L.end[k] <= i) ++k;
-    const long long j = i - (k ? L.end[k - 1] : 0);
-    const float g = L.g[k][j];
-    float m = L.m[k][j], v = L.v[k][j];
-    m = fmaf(1.0f - b1, g - m, m);
-    v = fmaf(1.0f - b2, g * g, b2 * v);
-    const float denom = sqrtf(v) * inv_sqrt_bc2 + eps;
-    L.p[k][j] -= lr_bc1 * (m / denom);
-    L.m[k][j] = m;
-    L.v[k][j] = v;
+  const int b = blockIdx.x;
+  int k = 0;
+  while (k < L.n - 1 && L.blk_end[k] <= b) ++k;
+  const long long base = k ? L.end[k - 1] : 0;
+  const long long numel = L.end[k] - base;
+  const long long j0 = (long long)(b - (k ? L.blk_end[k - 1] : 0)) * kAdamChunk + 4 * threadIdx.x;
+  float* P = L.p[k];
+  const float* G = L.g[k];
+  float* Mv = L.m[k];
+  float* V = L.v[k];
+  if (L.vec[k] && j0 + 3 < numel) {
+    const float4 g = *reinterpret_cast<const float4*>(G + j0);
+    float4 m = *reinterpret_cast<const float4*>(Mv + j0), v = *reinterpret_cast<const float4*>(V + j0);
+    float4 p = *reinterpret_cast<const float4*>(P + j0);
+    adam_elem(g.x, m.x, v.x, p.x, lr_bc1, b1, b2, inv_sqrt_bc2, eps);
+    adam_elem(g.y, m.y, v.y, p.y, lr_bc1, b1, b2, inv_sqrt_bc2, eps);
+    adam_elem(g.z, m.z, v.z, p.z, lr_bc1, b1, b2, inv_sqrt_bc2, eps);
+    adam_elem(g.w, m.w, v.w, p.w, lr_bc1, b1, b2, inv_sqrt_bc2, eps);
+    *reinterpret_cast<float4*>(P + j0) = p;
+    *reinterpret_cast<float4*>(Mv + j0) = m;
+    *reinterpret_cast<float4*>(V + j0) = v;
+  } else {
+    for (int q = 0; q < 4; ++q) {
+      const long long j = j0 + q;
+      if (j < numel) {
+        float m = Mv[j], v = V[j], p = P[j];
+        adam_elem(G[j], m, v, p, lr_bc1, b1, b2, inv_sqrt_bc2, eps);
+        P[j] = p;
+        Mv[j] = m;
+        V[j] = v;
+      }
+    }
   }
 }
 
@@ -88,6 +126,12 @@ static int make_list(float* const* params, const float* const* grads, float* con
     L->v[k] = exp_avg_sq[k];
     *total += numels[k];
     L->end[k] = *total;
+    const long long blocks = (numels[k] + kAdamChunk - 1) / kAdamChunk;
+    const long long prev = k ? L->blk_end[k - 1] : 0;
+    if (prev + blocks >= (1ll << 31)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+    L->blk_end[k] = int(prev + blocks);
+    L->vec[k] = pty_aligned(params[k], 16) && pty_aligned(grads[k], 16) && pty_aligned(exp_avg[k], 16) &&
+                pty_aligned(exp_avg_sq[k], 16);
   }
   L->n = n_tensors;
   return PTYCHO_OK;
@@ -108,11 +152,8 @@ extern "C" int ptycho_adam_step_dev(float* const* params, const float* const* gr
   if (st) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   k_adam_tick<<<1, 1, 0, s>>>(step);
-  if (total > 0) {
-    const long long blocks = (total + 255) / 256;
-    const int grid = (int)(blocks < 148 * 16 ? blocks : 148 * 16);
-    k_adam_dev<<<grid, 256, 0, s>>>(L, total, step, lr, beta1, beta2, eps);
-  }
+  if (total > 0 && L.blk_end[n_tensors - 1] > 0)
+    k_adam_dev_chunked<<<L.blk_end[n_tensors - 1], 256, 0, s>>>(L, step, lr, beta1, beta2, eps);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
