@@ -292,19 +292,23 @@ def test_fused_loss_autograd(pkg):
     assert rel_max(Pt.grad.cpu().numpy(), 3 * r["dP"]) <= 2e-4
 
 
-def test_fused_loss_backward_one_input_twice(pkg):
-    """Only the object needs a gradient; a retained graph backs up twice and the
-    scaled copies leave the saved gradients intact (accumulates 2 x 0.5 dO)."""
+@pytest.mark.parametrize("which", ["object", "probe"])
+def test_fused_loss_backward_one_input_twice(pkg, which):
+    """Only one input needs a gradient; a retained graph backs up twice and the
+    scaled copies leave the saved gradients intact (accumulates 2 x 0.5 d)."""
     dev = torch.device("cuda")
     O, P, tlY, tlX, Imeas = _case(64, 120, 5, seed=17)
-    Ot = torch.from_numpy(O).to(dev).requires_grad_(True)
-    Pt = torch.from_numpy(P).to(dev)
+    Ot = torch.from_numpy(O).to(dev).requires_grad_(which == "object")
+    Pt = torch.from_numpy(P).to(dev).requires_grad_(which == "probe")
     loss = pkg.fused_loss(Ot, Pt, pkg.make_windows(tlY, tlX, dev), torch.from_numpy(Imeas).to(dev),
                           "Poisson_likelihood_loss")
     (0.5 * loss).backward(retain_graph=True)
     (0.5 * loss).backward()
     r = fm.fwd_adj(O, P, tlY, tlX, Imeas, "Poisson_likelihood_loss")
-    assert rel_max(Ot.grad.cpu().numpy(), r["dO"]) <= 2e-4
+    if which == "object":
+        assert rel_max(Ot.grad.cpu().numpy(), r["dO"]) <= 2e-4 and Pt.grad is None
+    else:
+        assert rel_max(Pt.grad.cpu().numpy(), r["dP"]) <= 2e-4 and Ot.grad is None
 
 
 def test_frame_id_batches(pkg):
