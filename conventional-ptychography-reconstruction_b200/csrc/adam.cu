@@ -189,7 +189,7 @@ extern "C" int ptycho_adam_step(float* const* params, const float* const* grads,
 // ---- chain rule through the fused loss: scaled copies of dO and dP --------
 // The fused forward/adjoint produces dL/dO and dL/dP for a unit upstream
 // gradient; autograd's backward multiplies both by the upstream scalar g
-// (a device float).  One grid-stride launch covers both arrays (float4 where
+// (the FP64 loss's gradient, a device double).  One grid-stride launch covers both arrays (float4 where
 // both pointers are 16-byte aligned), out of place so the saved gradients stay
 // valid for a second backward.
 namespace pty {
@@ -197,8 +197,8 @@ namespace gsc {
 
 __global__ void __launch_bounds__(256) k_scale_pair(const float* __restrict__ a, float* __restrict__ ao, long long na,
                                                     const float* __restrict__ b, float* __restrict__ bo, long long nb,
-                                                    const float* __restrict__ g, int vec_a, int vec_b) {
-  const float s = __ldg(g);
+                                                    const double* __restrict__ g, int vec_a, int vec_b) {
+  const float s = float(__ldg(g));
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long qa = vec_a ? na / 4 : 0, qb = vec_b ? nb / 4 : 0;
@@ -218,16 +218,20 @@ __global__ void __launch_bounds__(256) k_scale_pair(const float* __restrict__ a,
 }  // namespace pty
 
 extern "C" int ptycho_scale_pair(const float* a, float* a_out, long long na, const float* b, float* b_out,
-                                 long long nb, const float* scale, ptycho_stream_t stream) {
+                                 long long nb, const double* scale, ptycho_stream_t stream) {
   if (!scale || na < 0 || nb < 0 || (na > 0 && (!a || !a_out)) || (nb > 0 && (!b || !b_out)))
     return PTYCHO_ERR_INVALID_ARG;
   if (!pty_aligned(a, 4) || !pty_aligned(a_out, 4) || !pty_aligned(b, 4) || !pty_aligned(b_out, 4) ||
-      !pty_aligned(scale, 4))
+      !pty_aligned(scale, 8))
     return PTYCHO_ERR_MISALIGNED;
   if (na + nb == 0) return PTYCHO_OK;
+  static int nsm_cache[64] = {};
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (dev >= 0 && dev < 64) {
+    if (nsm_cache[dev] == 0) cudaDeviceGetAttribute(&nsm_cache[dev], cudaDevAttrMultiProcessorCount, dev);
+    nsm = nsm_cache[dev] > 0 ? nsm_cache[dev] : 148;
+  }
   const long long work = (na + nb) / 4 + 1;
   const long long want = (work + 255) / 256;
   const int grid = int(want < 8LL * nsm ? want : 8LL * nsm);

@@ -318,15 +318,24 @@ template <int M, int MODE, int LOSS>
 int launch_fused_t(const FusedArgs& a, cudaStream_t s) {
   constexpr size_t smem = FusedSmem<M>::total;
   auto kern = k_fused<M, MODE, LOSS>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-    return PTYCHO_ERR_LAUNCH;
-  int dev = 0, nsm = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Plan<M>::NT, smem) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  const int slots = nsm * per_sm;
+  // the shared-memory attribute and the resident-CTA count are set up once per
+  // device (a per-call host cost otherwise); 0 = not yet known
+  constexpr int kMaxDev = 64;
+  static int slots_cache[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return PTYCHO_ERR_LAUNCH;
+  int slots = slots_cache[dev];
+  if (slots == 0) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+      return PTYCHO_ERR_LAUNCH;
+    int nsm = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Plan<M>::NT, smem) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    slots = nsm * per_sm;
+    slots_cache[dev] = slots;
+  }
   const int grid = a.B < slots ? a.B : slots;
   kern<<<grid, Plan<M>::NT, smem, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;

@@ -79,8 +79,22 @@ def check_windows(tl: torch.Tensor, canvas_hw, M: int) -> None:
 # --------------------------------------------------------------------------
 # raw calls
 # --------------------------------------------------------------------------
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def _stream_handle(device: torch.device) -> int:
+    """The current stream of ``device`` as a raw handle (a per-call host cost:
+    the direct accessor skips building a Stream object)."""
+    if _raw_stream is not None and device.index is not None:
+        return _raw_stream(device.index)
     return torch.cuda.current_stream(device).cuda_stream
+
+
+def _i32(x: torch.Tensor, dev) -> torch.Tensor:
+    """x as a contiguous int32 tensor on dev (no conversion call when it already is)."""
+    if x.dtype == torch.int32 and x.device == dev and x.is_contiguous():
+        return x
+    return x.to(device=dev, dtype=torch.int32).contiguous()
 
 
 def _as_c64(x: torch.Tensor, name: str) -> torch.Tensor:
@@ -103,6 +117,9 @@ _status_cache: dict = {}
 
 def device_status(device) -> torch.Tensor:
     """The per-device int32 status word the kernels raise errors into."""
+    st = _status_cache.get(device)
+    if st is not None:
+        return st
     device = torch.device(device)
     if device.index is None:
         device = torch.device(device.type, torch.cuda.current_device())
@@ -136,12 +153,13 @@ class FwdAdjWorkspace:
 
 
 _default_ws: dict = {}
+_ws_size_cache: dict = {}  # (H, W, M, B) -> ptycho_fwd_adj_workspace_size
 
 
 def _batch_arg(batch, dev):
     if batch is None:
         return None
-    return torch.as_tensor(batch).to(device=dev, dtype=torch.int32).contiguous()
+    return _i32(batch if isinstance(batch, torch.Tensor) else torch.as_tensor(batch), dev)
 
 
 def forward_intensity(O: torch.Tensor, P: torch.Tensor, tl: torch.Tensor, batch=None) -> torch.Tensor:
@@ -180,7 +198,7 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
     M = _check_probe(P)
     H, W = O.shape
     dev = O.device
-    tl = tl.to(device=dev, dtype=torch.int32).contiguous()
+    tl = _i32(tl, dev)
     F = int(tl.shape[0])
     if Imeas.dtype != torch.float32 or not Imeas.is_contiguous() or Imeas.device != dev:
         Imeas = Imeas.to(device=dev, dtype=torch.float32).contiguous()
@@ -188,6 +206,7 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
         raise ValueError(f"measurements must be [F, M, M] = {(F, M, M)}, got {tuple(Imeas.shape)}")
     bt = _batch_arg(batch, dev)
     B = F if bt is None else int(bt.numel())
+    stream = _stream_handle(dev)
     loss_total = torch.empty((), dtype=torch.float64, device=dev)
     lp = torch.empty(B, dtype=torch.float64, device=dev) if per_pattern else None
     if want_grad:
@@ -197,11 +216,16 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
             dP = torch.empty((M, M), dtype=torch.complex64, device=dev)
     else:
         dO = dP = None
-    ws_bytes = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, M, B))
+    key = (H, W, M, B)
+    ws_bytes = _ws_size_cache.get(key)
+    if ws_bytes is None:
+        ws_bytes = _ws_size_cache[key] = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, M, B))
     if workspace is None:
         # one default workspace per (device, stream): calls on one stream are
         # ordered, calls on different streams must not share scratch
-        workspace = _default_ws.setdefault((dev, _stream_handle(dev)), FwdAdjWorkspace())
+        workspace = _default_ws.get((dev, stream))
+        if workspace is None:
+            workspace = _default_ws.setdefault((dev, stream), FwdAdjWorkspace())
     ws = workspace.get(ws_bytes, dev)
     st = device_status(dev)
     _lib.check(_lib.lib().ptycho_fwd_adj(
@@ -209,8 +233,7 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
         bt.data_ptr() if bt is not None else None, B, int(loss_code),
         lp.data_ptr() if lp is not None else None, loss_total.data_ptr(),
         dO.data_ptr() if dO is not None else None, dP.data_ptr() if dP is not None else None,
-        1 if accumulate else 0, ws.data_ptr(), ws.numel(), st.data_ptr(),
-        _stream_handle(dev)), "ptycho_fwd_adj")
+        1 if accumulate else 0, ws.data_ptr(), ws.numel(), st.data_ptr(), stream), "ptycho_fwd_adj")
     return loss_total, lp, dO, dP
 
 
@@ -300,7 +323,7 @@ class _FusedLoss(torch.autograd.Function):
         if not ctx.need:
             return None, None, None, None, None, None
         dO, dP = ctx.saved_tensors
-        s = g.to(torch.float32).contiguous()
+        s = g if g.dtype == torch.float64 and g.is_contiguous() else g.to(torch.float64).contiguous()
         gO = torch.empty_like(dO) if ctx.needs_input_grad[0] else None
         gP = torch.empty_like(dP) if ctx.needs_input_grad[1] else None
         # one launch scales both gradients by the upstream scalar (out of place:
@@ -309,7 +332,7 @@ class _FusedLoss(torch.autograd.Function):
         _lib.check(_lib.lib().ptycho_scale_pair(
             ptr(dO if gO is not None else None), ptr(gO), 2 * dO.numel() if gO is not None else 0,
             ptr(dP if gP is not None else None), ptr(gP), 2 * dP.numel() if gP is not None else 0,
-            s.data_ptr(), torch.cuda.current_stream(s.device).cuda_stream), "ptycho_scale_pair")
+            s.data_ptr(), _stream_handle(s.device)), "ptycho_scale_pair")
         return gO, gP, None, None, None, None
 
 

@@ -236,13 +236,13 @@ int ptycho_adam_step_dev(float* const* params, const float* const* grads, float*
 
 /* ---------------------------------------------------------------------- *
  * Chain rule through the fused loss: a_out = g * a (na floats) and
- * b_out = g * b (nb floats) in one launch, g = *scale a device float (the
- * upstream gradient autograd hands the fused loss's backward).  Used for dO
+ * b_out = g * b (nb floats) in one launch, g = *scale a device double (the
+ * upstream gradient autograd hands the fused loss's FP64 output).  Used for dO
  * and dP (complex64 as their float views).  No counterpart in the reference,
  * where autograd scales each gradient inside its own backward graph.
  * ---------------------------------------------------------------------- */
 int ptycho_scale_pair(const float* a, float* a_out, long long na, const float* b, float* b_out,
-                      long long nb, const float* scale, ptycho_stream_t stream);
+                      long long nb, const double* scale, ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
  * Residual composition of the INR output, apply_residual of
