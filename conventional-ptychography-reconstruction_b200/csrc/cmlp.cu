@@ -25,7 +25,7 @@
 //   sum_c G_y_c^T [h3 | 1]_c
 // in TMEM across all its tiles (the appended ones column yields the bias
 // gradients).  Each CTA writes its raw accumulators once; k_cmlp_reduce sums
-// the CTA partials in CTA order and folds the real-form blocks back into
+// the CTA partials in a fixed order and folds the real-form blocks back into
 // complex gradients (G_W = (P+S) + i(R-Q) for [[P,Q],[R,S]]) -- deterministic,
 // no atomics.  Gradients follow torch's complex convention.
 #include <cuda_bf16.h>
@@ -509,12 +509,15 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
   if (w == 0) tc::tmem_free(tm, NCOLS);
 }
 
-// sum the CTA partials in CTA order and fold the real-form blocks
+// sum the CTA partials in a fixed order and fold the real-form blocks
+// Block b owns outputs 32 b .. 32 b + 31, one per lane, so each warp's loads of
+// one partial touch neighbouring raw entries; warp k sums partials k, k + 8, ...
+// in order and the eight warp sums are added in warp order.
 __global__ void __launch_bounds__(256) k_cmlp_reduce(const float* __restrict__ part, int nparts,
                                                      float* __restrict__ grad) {
-  const int e = blockIdx.x * 8 + (threadIdx.x >> 5);  // one warp per output
-  const int lane = threadIdx.x & 31;
-  if (e >= kGradFloats) return;
+  __shared__ float wsum[8][32];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int e = blockIdx.x * 32 + lane;
   // each output is a (sign-weighted) sum of at most two raw entries
   int i0 = -1, i1 = -1;
   float s1 = 0.f;
@@ -562,19 +565,35 @@ __global__ void __launch_bounds__(256) k_cmlp_reduce(const float* __restrict__ p
   } else if (e >= G_BO) {
     i0 = R_BO + (e - G_BO);
   }
-  // lane j sums partials j, j+32, ... in order; then a fixed xor tree
   float acc = 0.f;
-  if (i0 >= 0) {
-    for (int p = lane; p < nparts; p += 32) {
+  if (e < kGradFloats && i0 >= 0) {
+    int p = wp;
+    for (; p + 24 < nparts; p += 32) {  // four partials' loads in flight, added in order
+      float v[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float* P = part + size_t(p + 8 * k) * kPartFloats;
+        v[k] = P[i0];
+        if (i1 >= 0) v[k] = fmaf(s1, P[i1], v[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc += v[k];
+    }
+    for (; p < nparts; p += 8) {
       const float* P = part + size_t(p) * kPartFloats;
       float v = P[i0];
       if (i1 >= 0) v = fmaf(s1, P[i1], v);
       acc += v;
     }
   }
+  wsum[wp][lane] = acc;
+  __syncthreads();
+  if (wp == 0 && e < kGradFloats) {
+    float t = 0.f;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) grad[e] = acc;
+    for (int k = 0; k < 8; ++k) t += wsum[k][lane];  // warps in order
+    grad[e] = t;
+  }
 }
 
 // pack torch-layout parameters into the kernel's bf16 operand blob + fp32 block
@@ -719,7 +738,7 @@ static int cmlp_backward(int planar, const void* packed, const float* x, const f
   int grid = 0;
   int st = cm::launch<true>(a, s, &grid);
   if (st) return st;
-  cm::k_cmlp_reduce<<<(cm::kGradFloats + 7) / 8, 256, 0, s>>>(static_cast<const float*>(workspace), grid,
+  cm::k_cmlp_reduce<<<(cm::kGradFloats + 31) / 32, 256, 0, s>>>(static_cast<const float*>(workspace), grid,
                                                                   grad);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
