@@ -332,3 +332,35 @@ def test_residual_composition_matches_torch(pkg, n):
         assert rel_max(out.detach().cpu().numpy(), ref.detach().cpu().numpy()) <= 1e-6
         assert rel_max(mm.grad.cpu().numpy(), m64.grad.cpu().numpy()) <= 1e-5
         assert abs(float(k.grad) - float(k64.grad)) <= 1e-5 * abs(float(k64.grad))
+
+
+def test_residual_plumbing_as_the_reference_self_test(pkg):
+    """The checks of models/complex_inr.py:368-556 (its __main__ self-test) on
+    the drop-in: complex, finite outputs; with initial images the residual flags
+    are set, the initials are buffers, k_object / k_probe are trainable real
+    scalars initialised to 1e-8; without them there are no k parameters and no
+    initial buffers."""
+    dev = torch.device("cuda")
+    kw = dict(output_width=128, output_height=128, downsample_factor=2, update_probe=True, first_omega_0=1.0,
+              hidden_omega_0=1.0, n_levels=16, n_features_per_level=2, log2_hashmap_size=16)
+    g = torch.Generator(device=dev).manual_seed(0)
+    obj_init = (torch.randn(128, 128, device=dev, generator=g) + 1j * torch.randn(128, 128, device=dev, generator=g)) * 0.01
+    probe_init = (torch.randn(128, 128, device=dev, generator=g) + 1j * torch.randn(128, 128, device=dev, generator=g)) * 0.01
+    m = pkg.ComplexINRModel2D(**kw, use_residual=True, object_initial=obj_init.to(torch.complex64),
+                              probe_initial=probe_init.to(torch.complex64)).to(dev)
+    obj, probe = m()
+    for t in (obj, probe):
+        assert torch.is_complex(t) and torch.isfinite(torch.view_as_real(t)).all()
+    buffers = dict(m.named_buffers())
+    trainable = {n for n, p in m.named_parameters() if p.requires_grad}
+    assert m.has_object_residual and m.has_probe_residual
+    assert "object_initial" in buffers and "probe_initial" in buffers
+    for name in ("k_object", "k_probe"):
+        k = getattr(m, name)
+        assert name in trainable and not torch.is_complex(k) and abs(float(k) - 1e-8) < 1e-10
+    m0 = pkg.ComplexINRModel2D(**kw, use_residual=True).to(dev)  # residual asked for, no initials
+    obj0, probe0 = m0()
+    assert torch.is_complex(obj0) and torch.isfinite(torch.view_as_real(obj0)).all()
+    assert not m0.has_object_residual and not m0.has_probe_residual
+    assert not [n for n, _ in m0.named_parameters() if n.startswith("k_")]
+    assert not [n for n, _ in m0.named_buffers() if n.endswith("_initial")]
