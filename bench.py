@@ -186,7 +186,9 @@ def parity_vs_cpu(pkg, work, first, dev):
     ref = fm.fwd_adj(work["obj"], work["probe"], work["tlY"][idx], work["tlX"][idx], work["Imeas"][idx],
                      w.loss_type)
     rn = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())  # noqa: E731
-    out["vs_fp64_oracle"] = {"loss_rel_err": abs(float(loss) - ref["loss_total"]) / abs(ref["loss_total"]),
+    I = pkg.forward_intensity(O, P, tl, batch=torch.from_numpy(idx).to(dev))
+    out["vs_fp64_oracle"] = {"intensity_rel_err": rn(I.cpu().numpy(), ref["I"]),
+                             "loss_rel_err": abs(float(loss) - ref["loss_total"]) / abs(ref["loss_total"]),
                              "dO_rel_err": rn(dO.cpu().numpy(), ref["dO"]),
                              "dP_rel_err": rn(dP.cpu().numpy(), ref["dP"])}
     out["note"] = "max |GPU - ref| / max |ref| on the CPU baseline's first sampled minibatch"
