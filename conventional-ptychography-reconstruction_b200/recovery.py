@@ -279,7 +279,7 @@ class Trainer:
 def build_model(cfg, canvas, probe_hw, probe_initial=None, device="cuda"):
     mt = cfg.get("model_type", "inr")
     if mt == "gaussian_field":
-        raise NotImplementedError("the Gaussian-field representation is not part of this build")
+        raise NotImplementedError("the Gaussian-field representation has no model here; its rasteriser is gsplat.GaussianRasterize2D")
     if mt == "pixel_grid":
         return PixelGrid((canvas, canvas), probe_hw).to(device)
     use_res = cfg.get("use_residual", False) and cfg.get("init_type", "initNone") != "initNone"

@@ -9,7 +9,7 @@ zhixuanh0710/conventional-ptychography-reconstruction:
   (models/complex_inr.py:130-145, called at :279, :294).  tiny-cuda-nn is an
   unpinned third-party dependency absent from the reference tree, so this is a
   restatement of the published Instant-NGP method (Mueller et al. 2022) with
-  this build's documented choices: level l has scale
+  these choices: level l has scale
   ``s_l = base * per_level_scale**l - 1`` and ``r_l = ceil(s_l) + 1`` vertices
   per axis; a coordinate x in [0,1] maps to ``x * s_l + 0.5``; the cell corner
   is its floor and the bilinear weights the fractional part; a level whose

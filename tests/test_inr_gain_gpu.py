@@ -5,7 +5,7 @@ Poisson noise, smooth_L1): the INR (HashGrid + complex MLP, trained by this
 library's kernels) and the pixel grid (object and probe as plain parameters on
 the same fused forward/adjoint) start from the same probe and train for the same
 number of epochs, with Adam at the learning rates of the c0 pixel-grid run
-(1e-2, decayed x0.3 every 40 epochs) and of the c2 INR run (1e-3).  Both are judged the same way:
+(1e-2, decayed x0.3 every 40 epochs) and of the c2 INR run (1e-3).  Both are scored the same way:
 - the data residual R = sum (sqrt(I) - sqrt(Imeas))^2 / sum Imeas over the whole
   stack (FP64); an INR result counts only within 1.1x of the pixel grid's R;
 - the object error against the ground truth in the high-coverage box, after the
