@@ -453,7 +453,8 @@ def run_ours(args):
 
 def time_to_residual(args):
     """Time-to-residual on workload c2 (1024^2 canvas, 128^2 probe, 28x28 raster,
-    smooth_L1, batch 10): the pixel grid (object and probe as plain parameters,
+    smooth_L1, batch 10; or --ttr-workload c3 / c4 with the settings of
+    TTR_SETTINGS and WORKLOADS_DESC): the pixel grid (object and probe as plain parameters,
     fused kernels, Adam lr 1e-2 decayed x0.3 every pg-epochs/5 epochs) trains
     for --pg-epochs epochs and sets the
     target = 1.1 x its final data residual R = sum (sqrt(I) - sqrt(Imeas))^2 /
@@ -467,13 +468,18 @@ def time_to_residual(args):
     pkg = importlib.import_module(PKG)
     rec = importlib.import_module(PKG + ".recovery")
     from oracle import torch_inr
-    work = pkg.synth.make_workload("c2", device=dev)
+    wl = args.ttr_workload
+    cfgw = TTR_SETTINGS[wl]
+    work = pkg.synth.make_workload(wl, device=dev)
+    w = work["workload"]
+    canvas, bsz, grid = w.canvas, cfgw["batch"], cfgw["grid"]
+    ds = canvas // grid
     stack = torch.from_numpy(work["Imeas"]).to(dev)
     tl = pkg.make_windows(work["tlY"], work["tlX"], dev)
     F, M = stack.shape[0], stack.shape[1]
     P0 = torch.from_numpy(work["probe"].astype(np.complex64)).to(dev) * float(np.sqrt(M * M))
-    pls = torch_inr.per_level_scale_for(512, 16, 16)
-    out = {"metric": "time-to-residual (pixel-grid x1.1)", "workload": WORKLOADS_DESC["c2"], "frames": F}
+    pls = torch_inr.per_level_scale_for(grid, 16, 16)
+    out = {"metric": "time-to-residual (pixel-grid x1.1)", "workload": WORKLOADS_DESC[wl], "frames": F}
     gt = torch.from_numpy(work["obj"].astype(np.complex64)).to(dev)
     box = pkg.accuracy.coverage_box(work["tlY"], work["tlX"], (M, M), tuple(gt.shape), 0.5)
 
@@ -504,9 +510,9 @@ def time_to_residual(args):
                 break
         return hist, reached, t_train
 
-    pg = rec.PixelGrid((1024, 1024), (M, M), probe_init=P0).to(dev)
+    pg = rec.PixelGrid((canvas, canvas), (M, M), probe_init=P0).to(dev)
     step = max(1, args.pg_epochs // 5)
-    tpg = rec.Trainer(pg, stack, tl, "smooth_L1_loss", 10, 1e-2, lr_decay_step=step, lr_decay_gamma=0.3)
+    tpg = rec.Trainer(pg, stack, tl, w.loss_type, bsz, 1e-2, lr_decay_step=step, lr_decay_gamma=0.3)
     hist, _, t_pg = timed(tpg, args.pg_epochs, 1e9, None)
     r_pg = hist[-1][2]
     r_pg = min(h[2] for h in hist[-max(1, len(hist) // 10):])  # converged tail
@@ -515,33 +521,42 @@ def time_to_residual(args):
                          "object_error": object_err(pg), "history": hist[:: max(1, len(hist) // 10)]}
     out["object_error_box"] = list(box)
     out["target_residual"] = target
-    cfg = dict(model_type="inr", downsample_factor=2, n_levels=16, log2_hashmap_size=18, base_resolution=16,
+    cfg = dict(model_type="inr", downsample_factor=ds, n_levels=16, log2_hashmap_size=cfgw["log2T"],
+               base_resolution=16,
                per_level_scale=pls, first_omega_0=10.0, hidden_omega_0=1.0, trainable_omega0=True,
                use_residual=True, init_type="initProbe")
     torch.manual_seed(0)  # the MLP initialisations (nn.Linear defaults) draw from torch's RNG
-    model = rec.build_model(cfg, 1024, (M, M), P0, dev)
-    tin = rec.Trainer(model, stack, tl, "smooth_L1_loss", 10, 1e-3)
+    model = rec.build_model(cfg, canvas, (M, M), P0, dev)
+    tin = rec.Trainer(model, stack, tl, w.loss_type, bsz, cfgw["lr"])
     hist, reached, t_in = timed(tin, args.inr_epochs, args.inr_cap_s, target)
     out["inr_b200_kernels"] = {"reached": reached is not None, "seconds_to_target": reached[1] if reached else None,
                                "epochs_to_target": reached[0] if reached else None,
                                "seconds": round(t_in, 3), "best_residual": min(h[2] for h in hist),
                                "object_error": object_err(model),
-                               "ms_per_minibatch": 1e3 * t_in / (len(hist) * -(-F // 10)),
+                               "ms_per_minibatch": 1e3 * t_in / (len(hist) * -(-F // bsz)),
                                "history": hist[:: max(1, len(hist) // 10)]}
 
     class RefTrainer:  # the reference loop, per frame, on this GPU
         def __init__(self):
             torch.manual_seed(0)
-            self.model = torch_inr.RefINR(1024, 2, M, 16, 18, 16, pls, 10.0, 1.0, probe_initial=P0).to(dev)
-            self.opt = torch.optim.Adam([p for p in self.model.parameters() if p.requires_grad], lr=1e-3)
+            self.model = torch_inr.RefINR(canvas, ds, M, 16, cfgw["log2T"], 16, pls, 10.0, 1.0,
+                                          probe_initial=P0).to(dev)
+            self.opt = torch.optim.Adam([p for p in self.model.parameters() if p.requires_grad], lr=cfgw["lr"])
             self.mmf = stack.permute(1, 2, 0).contiguous()
             self.rng = np.random.default_rng(0)
+            self.t_start = None
+            self.minibatches = 0
 
         def epoch(self):
+            if self.t_start is None:
+                self.t_start = time.perf_counter()
             perm = self.rng.permutation(F)
-            for s0 in range(0, F, 10):
+            for s0 in range(0, F, bsz):
                 torch_inr.ref_minibatch(self.model, self.opt, self.mmf, work["tlY"], work["tlX"],
-                                        perm[s0:s0 + 10], "smooth_L1_loss")
+                                        perm[s0:s0 + bsz], w.loss_type)
+                self.minibatches += 1
+                if time.perf_counter() - self.t_start > args.ref_cap_s:
+                    break  # one reference epoch of c4 runs past the cap
 
         @torch.no_grad()
         def residual(self):
@@ -562,7 +577,7 @@ def time_to_residual(args):
                                   "seconds_to_target": reached[1] if reached else None,
                                   "epochs_to_target": reached[0] if reached else None,
                                   "seconds": round(t_ref, 3), "best_residual": min(h[2] for h in hist),
-                                  "ms_per_minibatch": 1e3 * t_ref / (len(hist) * -(-F // 10)),
+                                  "ms_per_minibatch": 1e3 * t_ref / max(1, ref.minibatches),
                                   "history": hist,
                                   "note": "reference ComplexINRModel2D/ComplexMLP and per-frame loop in torch "
                                           "(torch.fft); tiny-cuda-nn replaced by a torch HashGrid restatement"}
@@ -576,7 +591,7 @@ def run_time_to_residual(args):
 def ttr_summary(out):
     """The time-to-residual result in a few keys (for the default bench line)."""
     a, b, pg = out["inr_b200_kernels"], out["inr_reference_torch"], out["pixel_grid"]
-    return {"metric": out["metric"], "workload": "c2 (1024^2 canvas, 128^2 probe, 784 frames, batch 10)",
+    return {"metric": out["metric"], "workload": out["workload"],
             "unit": "s", "higher_is_better": False,
             "pixel_grid": {"epochs": pg["epochs"], "seconds": pg["seconds"], "residual": pg["residual"],
                            "object_error": pg["object_error"]},
@@ -870,7 +885,17 @@ def run_aux(args):
 
 WORKLOADS_DESC = {"c2": "c2: 1024^2 canvas, 128^2 probe, 28x28 raster (784 frames), smooth_L1, batch 10; INR "
                         "16 levels x 2, log2 T 18, base 16, finest 512, 512^2 object grid (ds 2), MLP 64x2, "
-                        "omega 10/1, probe initProbe + residual"}
+                        "omega 10/1, probe initProbe + residual",
+                  "c3": "c3: 2048^2 object, 256^2 probe, 48x48 raster (2304 frames), Poisson, 1e3 photons, "
+                        "batch 64; INR 16 levels x 2, log2 T 19, base 16, finest 1024, 1024^2 object grid (ds 2), "
+                        "MLP 64x2, omega 10/1, probe INR + initProbe residual",
+                  "c4": "c4: 4096^2 object, 256^2 probe, 96x96 raster (9216 frames), Poisson, 1e3 photons, "
+                        "batch 512; INR 16 levels x 2, log2 T 20, base 16, finest 2048, 2048^2 object grid (ds 2), "
+                        "MLP 64x2, omega 10/1, probe INR + initProbe residual"}
+# per workload: INR object grid (canvas / ds), log2 hash-table size, minibatch, INR learning rate
+TTR_SETTINGS = {"c2": dict(grid=512, log2T=18, batch=10, lr=1e-3),
+                "c3": dict(grid=1024, log2T=19, batch=64, lr=1e-3),
+                "c4": dict(grid=2048, log2T=20, batch=512, lr=1e-3)}
 
 
 def main():
@@ -884,6 +909,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-batch", type=int, default=0)
     ap.add_argument("--time-to-residual", action="store_true")
+    ap.add_argument("--ttr-workload", choices=sorted(TTR_SETTINGS), default="c2",
+                    help="workload of the time-to-residual protocol")
     ap.add_argument("--inr-step", action="store_true")
     ap.add_argument("--pg-epochs", type=int, default=200)
     ap.add_argument("--inr-epochs", type=int, default=2000)

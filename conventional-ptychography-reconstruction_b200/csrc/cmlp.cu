@@ -10,7 +10,10 @@
 //   y  = Wo h3 + bo (complex 1x32).
 // A complex layer acts on [Re h; Im h] as the real 64x64 block [[A,-B],[B,A]]
 // (W = A + iB).  Operands are BF16 in shared memory, accumulators FP32 in
-// tensor memory; one CTA handles tiles of 128 coordinates and loops over
+// tensor memory; the hidden activations entering layer 2, layer 3 and the
+// output layer are split into bf16(h) + bf16(h - bf16(h)), two MMAs into one
+// accumulator (with h rounded once to BF16, training on 1e3-photon Poisson data
+// stalled at about 3x the residual an FP32 MLP reached); one CTA handles tiles of 128 coordinates and loops over
 // tiles (persistent).  256 threads: warp w reads TMEM lane quarter w & 3 (tile
 // rows 32 (w & 3) .. +31) and does the elementwise work of half w >> 2 of each
 // layer's complex units, so the sin / cos / exp chains between two MMAs are
@@ -62,8 +65,15 @@ constexpr int S_ACT_END = S_GZ + 16 * GRP;
 // FP32 h2, h3 of the tile (backward only): [layer][re, im][32 units][128 rows],
 // kept from the forward recompute for the layer-3 and layer-2 gradients
 constexpr int S_HF = S_ACT_END;
-constexpr int kSmemBwd = S_HF + 2 * 2 * 32 * 128 * 4;  // 201888 bytes: one CTA per SM
-constexpr int kSmemFwd = S_GY;       // 91264 bytes: the forward needs x, h, h3 only -> two CTAs per SM
+// BF16 residuals h - bf16(h) of the input of layer 2, 3 or the output layer (8
+// groups, rewritten layer by layer): each of those MMAs runs once on bf16(h) and
+// once on the residual into the same accumulator, so the hidden activations
+// reach the tensor core with about 16 significant bits instead of 8
+constexpr int S_LO_BWD = int(pty_align_up_c(S_HF + 2 * 2 * 32 * 128 * 4, 1024));
+constexpr int kSmemBwd = S_LO_BWD + 8 * GRP;  // 219136 bytes: one CTA per SM
+constexpr int S_LO_FWD = S_GY;                // the forward needs x, h, h3 and the residual plane only
+constexpr int kSmemFwd = S_LO_FWD + 8 * GRP;  // 107648 bytes: two CTAs per SM
+static_assert(kSmemBwd <= 232448 && 2 * (kSmemFwd + 1024) <= 233472, "shared-memory budget");
 
 // every MMA footprint used below stays inside [0, S_ACT_END)
 static_assert(S_GY + 16 * GRP <= S_ACT_END, "output-grad A footprint");
@@ -104,6 +114,18 @@ PTY_DEVI void st8(unsigned char* base, int c, int f0, const float* v) {
   q.z = pack_bf16x2(v[4], v[5]);
   q.w = pack_bf16x2(v[6], v[7]);
   *reinterpret_cast<uint4*>(base + cm_off(c, f0)) = q;
+}
+// the same 8 values as bf16(v) at feature f0 of `hi` and as bf16(v - bf16(v))
+// at feature f_lo of `lo`
+PTY_DEVI void st8_split(unsigned char* hi, int f0, unsigned char* lo, int f_lo, int c, const float* v) {
+  float h[8], r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    h[k] = __bfloat162float(__float2bfloat16_rn(v[k]));
+    r[k] = v[k] - h[k];
+  }
+  st8(hi, c, f0, h);
+  st8(lo, c, f_lo, r);
 }
 
 // sin and cos of a after Cody-Waite reduction by 2 pi (two-constant split of
@@ -164,6 +186,7 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
   float* par = reinterpret_cast<float*>(sm + S_PAR);
   float* red = reinterpret_cast<float*>(sm + S_RED);
   float* hf = reinterpret_cast<float*>(sm + S_HF);  // valid in the backward only
+  constexpr int S_LO = BWD ? S_LO_BWD : S_LO_FWD;
   auto hfi = [&](int layer, int part, int unit) { return ((layer * 2 + part) * 32 + unit) * 128 + row; };
   constexpr uint32_t NCOLS = BWD ? kColsBwd : kColsFwd;
   const uint32_t sbase = tc::smem_addr(sm);
@@ -258,13 +281,16 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
       tc::ld16(tm + lo + T_D1 + 16 * h, d);
 #pragma unroll
       for (int k = 0; k < 16; ++k) sincos_rr(w1 * (d[k] + par[P_B1 + 16 * h + k]), &hi[k], &hr[k]);
-      st8(sm + S_H, row, 64 + 16 * h, hr);
-      st8(sm + S_H, row, 72 + 16 * h, hr + 8);
-      st8(sm + S_H, row, 96 + 16 * h, hi);
-      st8(sm + S_H, row, 104 + 16 * h, hi + 8);
+      st8_split(sm + S_H, 64 + 16 * h, sm + S_LO, 16 * h, row, hr);
+      st8_split(sm + S_H, 72 + 16 * h, sm + S_LO, 8 + 16 * h, row, hr + 8);
+      st8_split(sm + S_H, 96 + 16 * h, sm + S_LO, 32 + 16 * h, row, hi);
+      st8_split(sm + S_H, 104 + 16 * h, sm + S_LO, 40 + 16 * h, row, hi + 8);
     }
     // -- complex layers 2 and 3 ------------------------------------------------
-    step([&] { gemm_act_w(tm + T_D2, sbase + S_H + 8 * GRP, sbase + S_W2, 64, 64, 64, false); });
+    step([&] {
+      gemm_act_w(tm + T_D2, sbase + S_H + 8 * GRP, sbase + S_W2, 64, 64, 64, false);
+      gemm_act_w(tm + T_D2, sbase + S_LO, sbase + S_W2, 64, 64, 64, true);
+    });
     if (abort) break;
     {
       const int h = hh;
@@ -284,12 +310,15 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
           hf[hfi(0, 1, 16 * h + k)] = hi[k];
         }
       }
-      st8(sm + S_H, row, 16 * h, hr);
-      st8(sm + S_H, row, 8 + 16 * h, hr + 8);
-      st8(sm + S_H, row, 32 + 16 * h, hi);
-      st8(sm + S_H, row, 40 + 16 * h, hi + 8);
+      st8_split(sm + S_H, 16 * h, sm + S_LO, 16 * h, row, hr);
+      st8_split(sm + S_H, 8 + 16 * h, sm + S_LO, 8 + 16 * h, row, hr + 8);
+      st8_split(sm + S_H, 32 + 16 * h, sm + S_LO, 32 + 16 * h, row, hi);
+      st8_split(sm + S_H, 40 + 16 * h, sm + S_LO, 40 + 16 * h, row, hi + 8);
     }
-    step([&] { gemm_act_w(tm + T_D3, sbase + S_H, sbase + S_W3, 64, 64, 64, false); });
+    step([&] {
+      gemm_act_w(tm + T_D3, sbase + S_H, sbase + S_W3, 64, 64, 64, false);
+      gemm_act_w(tm + T_D3, sbase + S_LO, sbase + S_W3, 64, 64, 64, true);
+    });
     if (abort) break;
     {
       const int h = hh;
@@ -309,13 +338,16 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
           hf[hfi(1, 1, 16 * h + k)] = hi[k];
         }
       }
-      st8(sm + S_H3, row, 16 * h, hr);
-      st8(sm + S_H3, row, 8 + 16 * h, hr + 8);
-      st8(sm + S_H3, row, 32 + 16 * h, hi);
-      st8(sm + S_H3, row, 40 + 16 * h, hi + 8);
+      st8_split(sm + S_H3, 16 * h, sm + S_LO, 16 * h, row, hr);
+      st8_split(sm + S_H3, 8 + 16 * h, sm + S_LO, 8 + 16 * h, row, hr + 8);
+      st8_split(sm + S_H3, 32 + 16 * h, sm + S_LO, 32 + 16 * h, row, hi);
+      st8_split(sm + S_H3, 40 + 16 * h, sm + S_LO, 40 + 16 * h, row, hi + 8);
     }
     // -- output layer ----------------------------------------------------------
-    step([&] { gemm_act_w(tm + T_DO, sbase + S_H3, sbase + S_WO, 16, 16, 64, false); });
+    step([&] {
+      gemm_act_w(tm + T_DO, sbase + S_H3, sbase + S_WO, 16, 16, 64, false);
+      gemm_act_w(tm + T_DO, sbase + S_LO, sbase + S_WO, 16, 16, 64, true);
+    });
     if (abort) break;
     if (hh == 0) {  // warp-uniform
       float d[16];

@@ -128,24 +128,34 @@ def bf16_round(a):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def bf16_split(a):
+    """bf16(a) + bf16(a - bf16(a)): a value as the sum of two BF16 operands."""
+    hi = bf16_round(a)
+    return hi + bf16_round(np.asarray(a) - hi)
+
+
 def _ident(a):
     return a
 
 
-def cmlp_forward(x, params, q=_ident):
+def cmlp_forward(x, params, q=_ident, qh=None):
     """params: dict with W1 [H,32] real, b1 [H] real, w1 (omega), Wh[i] [H,H] complex,
     bh[i] [H] complex, wh[i], Wo [1,H] complex, bo [1] complex.  Returns y [N] and a cache.
-    ``q`` rounds every matmul operand (``bf16_round`` mirrors the BF16 tensor-core kernel)."""
+    ``q`` rounds every matmul operand and ``qh`` (default ``q``) the hidden
+    activations entering layer 2, layer 3 and the output layer in the forward;
+    ``q=bf16_round, qh=bf16_split`` mirrors the tensor-core kernel, whose weight
+    gradients use the single BF16 rounding of those activations."""
+    qh = q if qh is None else qh
     x = np.asarray(x, dtype=np.float64)
     z1 = q(x) @ q(params["W1"]).T + params["b1"]
     h = np.exp(1j * params["w1"] * z1)
     cache = {"x": x, "z": [z1], "h": [h], "q": q}
     for W, b, w in zip(params["Wh"], params["bh"], params["wh"]):
-        z = q(h) @ q(W).T + b
+        z = qh(h) @ q(W).T + b
         h = np.exp(1j * w * z)
         cache["z"].append(z)
         cache["h"].append(h)
-    y = (q(h) @ q(params["Wo"]).T + params["bo"])[:, 0]
+    y = (qh(h) @ q(params["Wo"]).T + params["bo"])[:, 0]
     return y, cache
 
 

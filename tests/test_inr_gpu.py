@@ -213,7 +213,7 @@ def test_cmlp_forward_backward_against_oracle(pkg, N):
     xt = torch.from_numpy(x).to(dev).requires_grad_(True)
     y = mlp.net(xt)
     assert y.shape == (N, 1) and y.dtype == torch.complex64
-    yq, cq = inr.cmlp_forward(x, params, q=inr.bf16_round)
+    yq, cq = inr.cmlp_forward(x, params, q=inr.bf16_round, qh=inr.bf16_split)
     y0, c0 = inr.cmlp_forward(x, params)
     yk = y.detach().cpu().numpy()[:, 0]
     assert rel_max(yk, yq) <= 5e-3, rel_max(yk, yq)
@@ -295,7 +295,7 @@ def test_complex_inr_model_matches_oracle_composition(pkg):
               "bh": [net[i].linear.bias.detach().cpu().numpy() for i in (1, 2)],
               "wh": [float(net[i].omega_0.detach()) for i in (1, 2)], "Wo": net[3].weight.detach().cpu().numpy(),
               "bo": net[3].bias.detach().cpu().numpy()}
-    y, _ = inr.cmlp_forward(feats, params, q=inr.bf16_round)
+    y, _ = inr.cmlp_forward(feats, params, q=inr.bf16_round, qh=inr.bf16_split)
     ref = inr.fourier_upsample(y.reshape(32, 32), 2)
     assert rel_max(obj.detach().cpu().numpy(), ref) <= 1e-2
     # training step runs through every kernel and gives finite gradients

@@ -33,7 +33,7 @@ def _rand(shape, seed):
 
 
 @pytest.mark.parametrize("h,w,s", [(64, 64, 2), (64, 256, 2), (128, 64, 4), (256, 256, 1),
-                                   (512, 512, 2), (1024, 512, 2), (2048, 256, 2)])
+                                   (512, 512, 2), (1024, 512, 2), (2048, 256, 2), (256, 2048, 2)])
 def test_forward_and_adjoint_against_oracle(pkg, h, w, s):
     dev = torch.device("cuda")
     x = _rand((h, w), h + w + s)
