@@ -216,6 +216,15 @@ class Trainer:
         self._graphs[n] = ent
         return ent
 
+    def prepare(self) -> None:
+        """Capture the graphs of an epoch's minibatch lengths now (full and, when
+        the frames do not divide evenly, the last one) instead of at their first
+        use; parameters and optimizer state are unchanged."""
+        if not self.use_graph or self.world > 1:
+            return
+        for n in {min(self.batch_size, self.F), self.F % self.batch_size} - {0}:
+            self._graph_for(n)
+
     def run(self, batch_ids: torch.Tensor) -> torch.Tensor:
         """One minibatch: replay of the captured step (or an eager step)."""
         if not self.use_graph:

@@ -34,17 +34,23 @@ def setup():
 def test_graph_and_eager_training_agree_bitwise(setup):
     pkg, rec, dev, stack, tl, H, M = setup
     res = []
-    for use_graph in (False, True):
+    # eager; graphs captured at first use; graphs captured up front by prepare()
+    # (30 frames in minibatches of 8: lengths 8 and 6)
+    for use_graph, prep in ((False, False), (True, False), (True, True)):
         torch.manual_seed(0)
         model = rec.PixelGrid((H, H), (M, M)).to(dev)
         tr = rec.Trainer(model, stack, tl, "Poisson_likelihood_loss", 8, 1e-2, lr_decay_step=1, lr_decay_gamma=0.5,
                          seed=3, use_graph=use_graph)
+        if prep:
+            tr.prepare()
+            assert sorted(tr._graphs) == [6, 8]
         for _ in range(3):
             tr.epoch()
         torch.cuda.synchronize()
         res.append([p.detach().clone() for p in model.parameters()])
-    for a, b in zip(*res):
-        assert torch.equal(a, b)
+    for other in res[1:]:
+        for a, b in zip(res[0], other):
+            assert torch.equal(a, b)
 
 
 def test_inr_training_lowers_residual(setup):
