@@ -63,6 +63,7 @@ def runs():
             obj, _ = model()
         err = pkg.accuracy.object_error(obj.reshape(C, C).to(torch.complex64), gt, box)
         out[name] = dict(r0=r0, r=tr.residual(), err=err["nrmse_scaled"])
+    print(f"\nc0, {EPOCHS} epochs each:", {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in out.items()})
     return out
 
 
