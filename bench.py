@@ -485,8 +485,11 @@ def time_to_residual(args):
 
     @torch.no_grad()
     def object_err(model):  # FP64 on the device, global phase (and complex factor) removed, coverage box
-        e = pkg.accuracy.object_error(model()[0].reshape(gt.shape).to(torch.complex64), gt, box)
-        return {"nrmse_phase": round(e["nrmse"], 5), "nrmse_scaled": round(e["nrmse_scaled"], 5)}
+        o = model()[0].reshape(gt.shape).to(torch.complex64)
+        e = pkg.accuracy.object_error(o, gt, box)
+        ea = pkg.accuracy.object_error_aligned(o, gt, box)  # after the sub-pixel translation as well
+        return {"nrmse_phase": round(e["nrmse"], 5), "nrmse_scaled": round(e["nrmse_scaled"], 5),
+                "nrmse_scaled_aligned": round(ea["nrmse_scaled"], 5), "shift": [round(v, 2) for v in ea["shift"]]}
 
     def timed(trainer, max_epochs, max_s, target):
         # garbage left by the previous arm (its CUDA graphs among it) is collected
@@ -647,7 +650,9 @@ def run_c0_reconstruction(args):
         Im = stack.double()
         r = float(((I.sqrt() - Im.sqrt()) ** 2).sum() / Im.sum())
         e = pkg.accuracy.object_error(obj, gt, box)
-        return r, {"nrmse_phase": round(e["nrmse"], 5), "nrmse_scaled": round(e["nrmse_scaled"], 5)}
+        ea = pkg.accuracy.object_error_aligned(obj, gt, box)
+        return r, {"nrmse_phase": round(e["nrmse"], 5), "nrmse_scaled": round(e["nrmse_scaled"], 5),
+                   "nrmse_scaled_aligned": round(ea["nrmse_scaled"], 5), "shift": [round(v, 2) for v in ea["shift"]]}
 
     pg = rec.PixelGrid((H, H), (M, M)).to(dev)
     tr = rec.Trainer(pg, stack, tl, w.loss_type, batch, lr)

@@ -262,6 +262,86 @@ def object_error(recon, gt, box=None):
     return e_phase, e_scaled
 
 
+def align_by_xcorr(recon_mag, gt_mag):
+    """Integer offset (row, col) of a recon inside a ground truth at least as large
+    (compare_object_ssim.py:75-89): the arg-max, over offsets that keep the recon
+    inside, of the circular cross-correlation of the mean-removed magnitudes with
+    the recon zero-padded to the truth's size; first maximum in row-major order."""
+    r = np.asarray(recon_mag, dtype=np.float64)
+    g = np.asarray(gt_mag, dtype=np.float64)
+    H, W = r.shape
+    Hg, Wg = g.shape
+    if Hg < H or Wg < W:
+        raise ValueError("ground truth smaller than the reconstruction")
+    rf = np.fft.fft2(r - r.mean(), s=(Hg, Wg))
+    gf = np.fft.fft2(g - g.mean(), s=(Hg, Wg))
+    xc = np.fft.ifft2(gf * np.conj(rf)).real[:Hg - H + 1, :Wg - W + 1]
+    i = np.unravel_index(int(np.argmax(xc)), xc.shape)
+    return int(i[0]), int(i[1])
+
+
+def _signed_freqs(n):
+    return np.fft.fftfreq(n) * n
+
+
+def register_translation(recon, gt, upsample=100):
+    """Sub-pixel shift d = (dy, dx) such that shift(recon, d) best matches gt, by
+    the upsampled-DFT cross-correlation of Guizar-Sicairos, Thurman and Fienup
+    (Opt. Lett. 33, 156, 2008): the FFT cross-correlation's peak locates d to the
+    pixel, then the correlation is evaluated by matrix DFTs on a 1/upsample grid
+    over +-0.75 pixel around it.  FP64 throughout."""
+    r = np.asarray(recon, dtype=np.complex128)
+    g = np.asarray(gt, dtype=np.complex128)
+    H, W = g.shape
+    X = np.fft.fft2(g) * np.conj(np.fft.fft2(r))
+    cc = np.abs(np.fft.ifft2(X))
+    py, px = np.unravel_index(int(np.argmax(cc)), cc.shape)
+    py = py - H if py > H // 2 else py
+    px = px - W if px > W // 2 else px
+    if upsample <= 1:
+        return float(py), float(px)
+    half = int(np.ceil(0.75 * upsample))
+    offs = np.arange(-half, half + 1) / upsample
+    ys, xs = py + offs, px + offs
+    Er = np.exp(2j * np.pi * np.outer(ys, _signed_freqs(H)) / H)
+    Ec = np.exp(2j * np.pi * np.outer(_signed_freqs(W), xs) / W)
+    up = np.abs(Er @ X @ Ec)
+    iy, ix = np.unravel_index(int(np.argmax(up)), up.shape)
+    return float(ys[iy]), float(xs[ix])
+
+
+def fourier_shift(img, dy, dx):
+    """img translated by (dy, dx) pixels, out(y, x) = img(y - dy, x - dx), periodic."""
+    a = np.asarray(img, dtype=np.complex128)
+    H, W = a.shape
+    ph = np.exp(-2j * np.pi * (np.outer(_signed_freqs(H) * dy / H, np.ones(W))
+                               + np.outer(np.ones(H), _signed_freqs(W) * dx / W)))
+    return np.fft.ifft2(np.fft.fft2(a) * ph)
+
+
+def register_in_box(recon, gt, box, upsample=100, iters=3):
+    """Shift aligning a canvas ``recon`` to ``gt`` inside ``box``: the crops'
+    mean is removed and a separable Hann window applied (the crops are not
+    periodic), ``register_translation`` is run on them, the shift is applied to
+    the whole canvas and the registration repeated on the shifted crop until the
+    increment is zero (at most ``iters`` times); the increments add up."""
+    y0, y1, x0, x1 = box
+
+    def win(a):
+        a = a - a.mean()
+        return a * np.outer(np.hanning(a.shape[0]), np.hanning(a.shape[1]))
+
+    g = win(np.asarray(gt, dtype=np.complex128)[y0:y1, x0:x1])
+    d = np.zeros(2)
+    for _ in range(iters):
+        rs = fourier_shift(recon, *d)[y0:y1, x0:x1]
+        dd = np.array(register_translation(win(rs), g, upsample))
+        d = d + dd
+        if not dd.any():
+            break
+    return float(d[0]), float(d[1])
+
+
 def coverage_box(tlY, tlX, probe_shape, canvas_shape, frac=0.5):
     """scan_coverage_mask + high_coverage_bbox (compare_object_ssim.py:42-72) on
     integer window corners: bbox of pixels covered >= ceil(frac * max) times."""

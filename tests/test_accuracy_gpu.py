@@ -65,3 +65,56 @@ def test_object_error_rejects_bad_input(acc):
         acc.object_error(a, torch.zeros(8, 9, dtype=torch.complex64, device=dev))
     with pytest.raises(Exception):
         acc.object_error(a, a, (0, 9, 0, 8))
+
+
+# ---- translation alignment (FP64 on the device) against the oracle -----------
+def _smooth(rng, H, W):
+    from scipy.ndimage import gaussian_filter
+    return gaussian_filter(rng.random((H, W)), 3) + 1j * gaussian_filter(rng.random((H, W)), 3)
+
+
+def test_align_by_xcorr_matches_oracle(acc):
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(21)
+    for Hg, Wg, H, W in ((64, 80, 40, 52), (128, 128, 128, 128), (90, 70, 31, 17)):
+        g = rng.random((Hg, Wg))
+        y, x = rng.integers(0, Hg - H + 1), rng.integers(0, Wg - W + 1)
+        r = g[y:y + H, x:x + W] * (1 + 0.05 * rng.random((H, W)))
+        got = acc.align_by_xcorr(torch.from_numpy(r).to(dev), torch.from_numpy(g).to(dev))
+        assert got == fm.align_by_xcorr(r, g) == (y, x)
+
+
+@pytest.mark.parametrize("d", [(0.0, 0.0), (0.37, -1.62), (-2.5, 3.01), (6.0, -0.99)])
+def test_register_translation_matches_oracle(acc, d):
+    """Same peak on the same 1/100 grid as the oracle; the shift found is the one applied."""
+    dev = torch.device("cuda")
+    g = _smooth(np.random.default_rng(5), 96, 112)
+    r = fm.fourier_shift(g, -d[0], -d[1])
+    got = acc.register_translation(torch.from_numpy(r).to(dev), torch.from_numpy(g).to(dev))
+    assert got == fm.register_translation(r, g, 100)
+    assert np.allclose(got, d, atol=1e-9)
+    back = acc.fourier_shift(torch.from_numpy(r).to(dev), *got).cpu().numpy()
+    assert np.abs(back - fm.fourier_shift(r, *got)).max() <= 1e-12 * np.abs(r).max()
+
+
+def test_object_error_aligned(acc):
+    """A truth shifted by a sub-pixel amount inside the box: the aligned error is
+    at FP32 round-off, the unaligned one is not; the box excludes the wrapped edges."""
+    dev = torch.device("cuda")
+    g = _smooth(np.random.default_rng(8), 160, 160)
+    r = (0.8 * np.exp(0.4j) * fm.fourier_shift(g, 1.23, -0.71)).astype(np.complex64)
+    box = (20, 140, 24, 136)
+    rt, gt = torch.from_numpy(r).to(dev), torch.from_numpy(g.astype(np.complex64)).to(dev)
+    e = acc.object_error_aligned(rt, gt, box)
+    assert np.allclose(e["shift"], (-1.23, 0.71), atol=1e-9)
+    assert np.allclose(e["shift"], fm.register_in_box(r, g, box), atol=1e-9)
+    assert e["nrmse_scaled"] < 1e-5, e
+    assert acc.object_error(rt, gt, box)["nrmse_scaled"] > 1e-2
+
+
+def test_alignment_rejects_host_tensors(acc):
+    a = torch.zeros(8, 8, dtype=torch.complex64)
+    with pytest.raises(ValueError):
+        acc.register_translation(a, a)
+    with pytest.raises(ValueError):
+        acc.align_by_xcorr(a.real, a.real)
