@@ -702,27 +702,31 @@ def run_c0_reconstruction(args):
 
 
 def run_inr_step(args):
-    """Throughput of one INR training minibatch on workload c2 (graph-replayed:
-    HashGrid forward, tcgen05 MLP forward, Fourier upsample, probe INR, fused
-    loss of 10 patterns, backward through all of them, fused Adam).  Reports
-    ms per minibatch and the MLP's tensor-core FLOP rate (forward 18.6 kflop
-    per coordinate, backward with the recomputed forward 3 x that)."""
+    """Throughput of one INR training minibatch on workload c2 (or --ttr-workload
+    c3 / c4 with the settings of TTR_SETTINGS), graph-replayed: HashGrid forward,
+    tcgen05 MLP forward, Fourier upsample, probe INR, fused loss of one
+    minibatch, backward through all of them, fused Adam.  Reports ms per
+    minibatch and the MLP's tensor-core FLOP rate (forward 18.6 kflop per
+    coordinate, backward with the recomputed forward 3 x that)."""
     dev = torch.device("cuda")
     pkg = importlib.import_module(PKG)
     rec = importlib.import_module(PKG + ".recovery")
     from oracle import torch_inr  # per-level scale formula only
-    work = pkg.synth.make_workload("c2", device=dev)
+    wl = args.ttr_workload
+    cfgw = TTR_SETTINGS[wl]
+    work = pkg.synth.make_workload(wl, device=dev)
+    w = work["workload"]
     stack = torch.from_numpy(work["Imeas"]).to(dev)
     tl = pkg.make_windows(work["tlY"], work["tlX"], dev)
-    M = stack.shape[1]
+    M, grid, bsz = stack.shape[1], cfgw["grid"], cfgw["batch"]
     P0 = torch.from_numpy(work["probe"].astype(np.complex64)).to(dev) * float(M)
-    cfg = dict(model_type="inr", downsample_factor=2, n_levels=16, log2_hashmap_size=18, base_resolution=16,
-               per_level_scale=torch_inr.per_level_scale_for(512, 16, 16), first_omega_0=10.0,
+    cfg = dict(model_type="inr", downsample_factor=w.canvas // grid, n_levels=16, log2_hashmap_size=cfgw["log2T"],
+               base_resolution=16, per_level_scale=torch_inr.per_level_scale_for(grid, 16, 16), first_omega_0=10.0,
                hidden_omega_0=1.0, trainable_omega0=True, use_residual=True, init_type="initProbe")
-    model = rec.build_model(cfg, 1024, (M, M), P0, dev)
-    tr = rec.Trainer(model, stack, tl, "smooth_L1_loss", 10, 1e-3)
+    model = rec.build_model(cfg, w.canvas, (M, M), P0, dev)
+    tr = rec.Trainer(model, stack, tl, w.loss_type, bsz, cfgw["lr"])
     g = torch.Generator(device=dev).manual_seed(0)
-    batches = [torch.randperm(stack.shape[0], device=dev, generator=g)[:10].to(torch.int32)
+    batches = [torch.randperm(stack.shape[0], device=dev, generator=g)[:bsz].to(torch.int32)
                for _ in range(args.warmup + args.steps)]
     for i in range(args.warmup):
         tr.run(batches[i])
@@ -735,10 +739,11 @@ def run_inr_step(args):
     e1.record(s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    coords = 512 * 512 + M * M
+    coords = grid * grid + M * M
     flops = coords * 18624 * 4  # forward + backward (recomputed forward + 2 GEMM passes)
-    print(json.dumps({"metric": "INR training minibatch (c2)", "ms_per_minibatch": ms, "steps": args.steps,
-                      "coordinates_per_minibatch": coords, "mlp_tflops_effective": flops / (ms * 1e-3) / 1e12,
+    print(json.dumps({"metric": f"INR training minibatch ({wl})", "ms_per_minibatch": ms, "steps": args.steps,
+                      "workload": WORKLOADS_DESC[wl], "coordinates_per_minibatch": coords,
+                      "mlp_tflops_effective": flops / (ms * 1e-3) / 1e12,
                       "note": "one CUDA-graph replay per minibatch; MLP flops counted as 4 x 18.6 kflop/coord"}),
           flush=True)
 
