@@ -178,27 +178,29 @@ PTY_DEVI float2 dfeat_at(const float* __restrict__ dfeat, int item, int N) {
   else return __ldg(reinterpret_cast<const float2*>(dfeat) + item);
 }
 
-// long segments (coarse levels): one warp per entry, lanes stride the segment
-// in order, fixed xor tree
-template <bool PLANAR>
+// long segments (coarse levels): a group of G lanes per entry (G = 32: one warp;
+// G = 8: four entries per warp, for hashed levels' segments of 16 to 31), lanes stride the
+// segment in order, fixed xor tree within the group.  Entries [e0, e1).
+template <bool PLANAR, int G>
 __global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ start, const int* __restrict__ item,
                                                        const float* __restrict__ weight,
-                                                       const float* __restrict__ dfeat, int N, int E,
+                                                       const float* __restrict__ dfeat, int N, int e0, int e1,
                                                        float2* __restrict__ dtable, int accumulate) {
-  const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (e >= E) return;
-  const int s0 = start[e], s1 = start[e + 1];
+  static_assert(G == 8 || G == 16 || G == 32, "lane group");
+  const int lane = threadIdx.x & 31, gl = lane % G;
+  const int e = e0 + (blockIdx.x * 8 + (threadIdx.x >> 5)) * (32 / G) + lane / G;
+  const bool in = e < e1;  // every lane stays for the shuffles
+  const int s0 = in ? start[e] : 0, s1 = in ? start[e + 1] : 0;
   float ax = 0.f, ay = 0.f;
-  int j = s0 + lane;
+  int j = s0 + gl;
   // four strides' loads in flight, then the adds in the same order as one at a time
-  for (; j + 96 < s1; j += 128) {
+  for (; j + 3 * G < s1; j += 4 * G) {
     float w[4];
     float2 g[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      w[k] = __ldg(weight + j + 32 * k);
-      g[k] = dfeat_at<PLANAR>(dfeat, __ldg(item + j + 32 * k), N);
+      w[k] = __ldg(weight + j + G * k);
+      g[k] = dfeat_at<PLANAR>(dfeat, __ldg(item + j + G * k), N);
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -206,18 +208,18 @@ __global__ void __launch_bounds__(256) k_hash_bwd_warp(const int* __restrict__ s
       ay = fmaf(w[k], g[k].y, ay);
     }
   }
-  for (; j < s1; j += 32) {
+  for (; j < s1; j += G) {
     const float w = __ldg(weight + j);
     const float2 g = dfeat_at<PLANAR>(dfeat, __ldg(item + j), N);
     ax = fmaf(w, g.x, ax);
     ay = fmaf(w, g.y, ay);
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
+  for (int o = G / 2; o > 0; o >>= 1) {
     ax += __shfl_xor_sync(0xffffffffu, ax, o);
     ay += __shfl_xor_sync(0xffffffffu, ay, o);
   }
-  if (lane == 0) {
+  if (in && gl == 0) {
     float2 r = make_float2(ax, ay);
     if (accumulate) {
       const float2 old = dtable[e];
@@ -341,17 +343,32 @@ static int hash_backward(bool planar, const int32_t* start, const int32_t* item,
   if (st) return st;
   if (N < 0 || !start || !item || !weight || !dfeatures || !dtable) return PTYCHO_ERR_INVALID_ARG;
   if (!pty_aligned(dfeatures, planar ? 4 : 8) || !pty_aligned(dtable, 8)) return PTYCHO_ERR_MISALIGNED;
-  // levels whose average segment is long go to the warp-per-entry kernel
-  int split = 0;
-  for (int l = 0; l < L.levels; ++l)
+  // by average segment length 4N / n_l (levels run coarse to fine, so each rule
+  // holds for a prefix): >= 32, or >= 16 on a dense level, a warp per entry;
+  // >= 16 on a hashed level eight lanes per entry; shorter a thread per entry
+  // (measured: eight lanes gained on 2^20-entry hashed levels with segments of
+  // 16 and lost on dense levels with segments of 16 to 31)
+  int split32 = 0, split = 0;
+  for (int l = 0; l < L.levels; ++l) {
+    const long long seg4 = (long long)N * 4;
+    if (seg4 >= 32ll * L.n[l] || (L.dense[l] && seg4 >= 16ll * L.n[l])) split32 = L.offset[l] + L.n[l];
     if ((long long)N * 4 >= 16ll * L.n[l]) split = L.offset[l] + L.n[l];
+  }
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   float2* dt = reinterpret_cast<float2*>(dtable);
-  if (split > 0) {
+  if (split32 > 0) {
+    const unsigned g = unsigned((split32 + 7) / 8);
     if (planar)
-      k_hash_bwd_warp<true><<<(split + 7) / 8, 256, 0, s>>>(start, item, weight, dfeatures, N, split, dt, accumulate);
+      k_hash_bwd_warp<true, 32><<<g, 256, 0, s>>>(start, item, weight, dfeatures, N, 0, split32, dt, accumulate);
     else
-      k_hash_bwd_warp<false><<<(split + 7) / 8, 256, 0, s>>>(start, item, weight, dfeatures, N, split, dt, accumulate);
+      k_hash_bwd_warp<false, 32><<<g, 256, 0, s>>>(start, item, weight, dfeatures, N, 0, split32, dt, accumulate);
+  }
+  if (split > split32) {
+    const unsigned g = unsigned((split - split32 + 31) / 32);  // 8 warps x 4 entries per block
+    if (planar)
+      k_hash_bwd_warp<true, 8><<<g, 256, 0, s>>>(start, item, weight, dfeatures, N, split32, split, dt, accumulate);
+    else
+      k_hash_bwd_warp<false, 8><<<g, 256, 0, s>>>(start, item, weight, dfeatures, N, split32, split, dt, accumulate);
   }
   if (L.total > split) {
     const unsigned g = (L.total - split + 255) / 256;
