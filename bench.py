@@ -45,6 +45,7 @@ PKG = "conventional-ptychography-reconstruction_b200"
 
 METRIC = "fwd+adj patterns/s"
 L2_FLUSH_BYTES = 256 << 20
+SETTLE_S = 0.6  # untimed steps on either side of the timed ones while clocks are sampled
 
 
 def algorithmic_bytes_per_pattern(M: int, B: int) -> float:
@@ -103,7 +104,7 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, note=None):
         if not self.path or not os.path.exists(self.path):
             return None
         sm, mx, reasons = [], None, set()
@@ -123,8 +124,11 @@ class ClockSampler:
         os.unlink(self.path)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+               "samples": len(sm)}
+        if note:
+            out["note"] = note
+        return out
 
 
 def dist_setup(n_gpus: int):
@@ -287,25 +291,47 @@ def run_ours(args):
         exchange.all_reduce(dO, dP)  # N > 1: dO over the scanned rows, dP (NCCL)
         return plan.loss_total
 
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record(s)
     for i in range(args.warmup):
         step(i)
         flush.zero_()
+    w1.record(s)
     torch.cuda.synchronize()
+    # The K timed steps last ~1 ms, shorter than nvidia-smi's sampling period,
+    # so the clock record spans them plus SETTLE_S of identical untimed steps
+    # on either side (same kernels, same flushes).  The count is agreed over
+    # ranks, so every rank takes the same collective steps.
+    n_settle = int(min(20000, max(1, SETTLE_S * 1e3 / max(w0.elapsed_time(w1) / max(args.warmup, 1), 1e-3))))
     if world > 1:
         import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
+        nt = torch.tensor([n_settle], dtype=torch.int64, device=dev)
+        dist.all_reduce(nt, op=dist.ReduceOp.MAX)
+        n_settle = int(nt)
+
+    def settle():
+        for i in range(n_settle):
+            step(i % nb)
+            flush.zero_()
+
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local) as clk:
+        settle()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(s)
             step(args.warmup + k)
             ev[k][1].record(s)
         torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        settle()
+        torch.cuda.synchronize()
     times = [a.elapsed_time(b) for a, b in ev]  # ms
     t_tot = torch.tensor([sum(times)], dtype=torch.float64, device=dev)
     if world > 1:
@@ -428,7 +454,9 @@ def run_ours(args):
                 "data": "synthetic (seeded generator; reference datasets not distributed)",
                 "config": _config(w, B, args), "roofline": roof, "e2e": e2e,
                 "e2e_resident_stack": e2e_resident, "gpu_launches": launches,
-                "clocks": clk.summary()}
+                "clocks": clk.summary(note=f"sampled every 50 ms over the {args.steps} timed steps and "
+                                           f"{n_settle} identical untimed steps on either side "
+                                           f"(~{SETTLE_S:.1f} s each)")}
         if world == 1 and not args.no_ttr and args.workload == "c1":
             # the headline's second half: time-to-residual, INR vs pixel grid (c2); run
             # before the CPU baseline, whose idle OpenMP workers would share the host

@@ -6,14 +6,13 @@ Same constructor, attributes (``xy_coords``, ``probe_coords``,
 The hash encoders are :class:`hashgrid.Encoding` (tiny-cuda-nn's interface),
 the MLPs :class:`cmlp.ComplexMLP` (fused tensor-core kernels) and the Fourier
 upsampling of the object (models/complex_inr.py:252-271) the shared-memory
-FFT resampling kernels of :mod:`resample` (power-of-two sizes; the torch.fft
-formula otherwise).
+FFT resampling kernels of :mod:`resample` (any size the reference's geometry
+gives: power-of-two and mixed-radix lines; no torch.fft path).
 """
 from __future__ import annotations
 
 import torch
 import torch.nn as nn
-import torch.nn.functional as F
 
 from . import _lib, resample
 from .cmlp import ComplexMLP
@@ -124,19 +123,20 @@ class ComplexINRModel2D(nn.Module):
             self.has_probe_residual = False
 
     def fourier_upsample(self, x, scale_factor):
-        """fftshift(fft2) -> zero-pad -> ifftshift -> ifft2, times scale^2 (:252-271).
-
-        Power-of-two sizes run on the resampling kernels (``resample``); other
-        shapes keep the reference's torch.fft formula."""
+        """fftshift(fft2) -> zero-pad -> ifftshift -> ifft2, times scale^2 (:252-271),
+        on the resampling kernels (``resample``) for every [B, C, H, W] slice.
+        The scale must be a whole number (Recovery.py coerces downsample_factor
+        to int); there is no torch.fft path, so other inputs raise."""
         B, C, H, W = x.shape
-        if B == 1 and C == 1 and x.is_cuda and resample.supported(H, W, scale_factor):
-            return resample.fourier_upsample(x[0, 0], int(scale_factor))[None, None]
-        x_fft = torch.fft.fftshift(torch.fft.fft2(x, dim=(-2, -1)), dim=(-2, -1))
-        nH, nW = int(H * scale_factor), int(W * scale_factor)
-        ph, pw = (nH - H) // 2, (nW - W) // 2
-        x_fft = F.pad(x_fft, (pw, nW - W - pw, ph, nH - H - ph), mode="constant", value=0)
-        x_up = torch.fft.ifft2(torch.fft.ifftshift(x_fft, dim=(-2, -1)), dim=(-2, -1))
-        return x_up * (scale_factor ** 2)
+        if int(scale_factor) != scale_factor:
+            raise ValueError(f"downsample_factor must be a whole number, got {scale_factor}")
+        s = int(scale_factor)
+        if not x.is_cuda or not resample.supported(H, W, s):
+            raise ValueError(f"fourier_upsample: unsupported input {tuple(x.shape)} on {x.device} with scale {s}")
+        if B == 1 and C == 1:
+            return resample.fourier_upsample(x[0, 0], s)[None, None]
+        return torch.stack([resample.fourier_upsample(x[b, c], s) for b in range(B) for c in range(C)]
+                           ).reshape(B, C, H * s, W * s)
 
     def forward(self):
         xy = self.xy_coords if self.xy_coords.is_cuda else self.xy_coords.cuda()

@@ -225,13 +225,14 @@ extern "C" int ptycho_scale_pair(const float* a, float* a_out, long long na, con
       !pty_aligned(scale, 8))
     return PTYCHO_ERR_MISALIGNED;
   if (na + nb == 0) return PTYCHO_OK;
-  static int nsm_cache[64] = {};
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64) {
-    if (nsm_cache[dev] == 0) cudaDeviceGetAttribute(&nsm_cache[dev], cudaDevAttrMultiProcessorCount, dev);
-    nsm = nsm_cache[dev] > 0 ? nsm_cache[dev] : 148;
+  static PtyDevCache nsm_cache;
+  int dev = 0;
+  int nsm = nsm_cache.get(&dev);
+  if (nsm == 0 && dev >= 0) {
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) nsm = 0;
+    nsm_cache.put(dev, nsm > 0 ? nsm : 0);
   }
+  if (nsm <= 0) nsm = 148;
   const long long work = (na + nb) / 4 + 1;
   const long long want = (work + 255) / 256;
   const int grid = int(want < 8LL * nsm ? want : 8LL * nsm);

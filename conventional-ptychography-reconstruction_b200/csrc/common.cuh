@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/ptycho_b200.h"
 
 #define PTY_DEVI __device__ __forceinline__
@@ -29,3 +31,28 @@ static inline bool pty_aligned(const void* p, size_t a) {
 }
 static inline size_t pty_align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 __host__ __device__ constexpr size_t pty_align_up_c(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Per-device cache of a launch set-up value that is computed once per device
+// (a resident-CTA count, an SM count, "the shared-memory attribute is set");
+// 0 means not yet known.  Entries are atomics, so host threads may race on
+// them: two threads that both miss compute and store the same value.  A
+// device reset drops a kernel's shared-memory attribute, so a launcher that
+// caches "attribute set" clears its entry and sets it again when a launch is
+// refused (static storage: every entry starts at 0).
+constexpr int kPtyMaxDevices = 64;
+struct PtyDevCache {
+  std::atomic<int> v[kPtyMaxDevices];
+  // the cached value of the current device, or 0; dev_out receives the device
+  int get(int* dev_out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kPtyMaxDevices) {
+      *dev_out = -1;
+      return 0;
+    }
+    *dev_out = dev;
+    return v[dev].load(std::memory_order_relaxed);
+  }
+  void put(int dev, int x) {
+    if (dev >= 0 && dev < kPtyMaxDevices) v[dev].store(x, std::memory_order_relaxed);
+  }
+};

@@ -5,7 +5,8 @@
 //   X[k] = sum_n a[n*S] * exp(-+ 2 pi i n k / R)   (minus: forward, plus: INV).
 // All indices are compile-time constants, so after inlining the arrays live in
 // registers.  Radix 16 is 4x4 Cooley-Tukey, radix 8 is 2x4; the internal
-// twiddles are the exact constants cos/sin(pi/8), cos/sin(pi/4).
+// twiddles are the exact constants cos/sin(pi/8), cos/sin(pi/4).  Radix 3, 5
+// and 7 use the symmetric pair form with exact cos/sin(2 pi q / P).
 #pragma once
 #include "common.cuh"
 
@@ -110,6 +111,59 @@ PTY_DEVI void dft16(float2* a) {
     for (int k2 = 0; k2 < 4; ++k2) a[(k1 + 4 * k2) * S] = t[4 * k1 + k2];
 }
 
+// exact cos / sin(2 pi q / P) for the odd primes 3, 5, 7 (q = 0 .. P-1)
+template <int P>
+__host__ __device__ constexpr float odd_cos(int q) {
+  q %= P;
+  if (q > P / 2) q = P - q;
+  if (q == 0) return 1.f;
+  if constexpr (P == 3) return -0.5f;
+  if constexpr (P == 5) return q == 1 ? 0.30901699437494742410f : -0.80901699437494742410f;
+  return q == 1 ? 0.62348980185873353053f : (q == 2 ? -0.22252093395631440429f : -0.90096886790241912624f);
+}
+template <int P>
+__host__ __device__ constexpr float odd_sin(int q) {
+  q %= P;
+  const float sg = q > P / 2 ? -1.f : 1.f;
+  if (q > P / 2) q = P - q;
+  if (q == 0) return 0.f;
+  if constexpr (P == 3) return sg * 0.86602540378443864676f;
+  if constexpr (P == 5) return sg * (q == 1 ? 0.95105651629515357212f : 0.58778525229247312917f);
+  return sg * (q == 1 ? 0.78183148246802980871f : (q == 2 ? 0.97492791218182360702f : 0.43388373911755812048f));
+}
+
+// odd prime P: pairs a_m +- a_{P-m} give, for r = 1 .. (P-1)/2,
+//   A_r = a_0 + sum_m (a_m + a_{P-m}) cos(2 pi m r / P)
+//   B_r =       sum_m (a_m - a_{P-m}) sin(2 pi m r / P)
+//   X_r = A_r -+ i B_r,  X_{P-r} = A_r +- i B_r   (upper sign: forward)
+template <int P, bool INV, int S>
+PTY_DEVI void dft_odd(float2* a) {
+  constexpr int h = (P - 1) / 2;
+  float2 sp[h], sm[h];
+  float2 x0 = a[0], sum = a[0];
+#pragma unroll
+  for (int m = 1; m <= h; ++m) {
+    sp[m - 1] = c_add(a[m * S], a[(P - m) * S]);
+    sm[m - 1] = c_sub(a[m * S], a[(P - m) * S]);
+    sum = c_add(sum, sp[m - 1]);
+  }
+#pragma unroll
+  for (int r = 1; r <= h; ++r) {
+    float2 A = x0, Bv = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = 1; m <= h; ++m) {
+      const float c = odd_cos<P>(m * r), s = odd_sin<P>(m * r);
+      A = make_float2(fmaf(sp[m - 1].x, c, A.x), fmaf(sp[m - 1].y, c, A.y));
+      Bv = make_float2(fmaf(sm[m - 1].x, s, Bv.x), fmaf(sm[m - 1].y, s, Bv.y));
+    }
+    // -i B = (B.y, -B.x); +i B = (-B.y, B.x)
+    const float2 mib = INV ? make_float2(-Bv.y, Bv.x) : make_float2(Bv.y, -Bv.x);
+    a[r * S] = c_add(A, mib);
+    a[(P - r) * S] = c_sub(A, mib);
+  }
+  a[0] = sum;
+}
+
 template <int R, bool INV, int S>
 PTY_DEVI void dft(float2* a) {
   if constexpr (R == 1) {
@@ -121,6 +175,8 @@ PTY_DEVI void dft(float2* a) {
     dft8<INV, S>(a);
   } else if constexpr (R == 16) {
     dft16<INV, S>(a);
+  } else if constexpr (R == 3 || R == 5 || R == 7) {
+    dft_odd<R, INV, S>(a);
   } else {
     static_assert(R == 16, "unsupported radix");
   }

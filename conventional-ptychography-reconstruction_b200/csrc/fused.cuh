@@ -319,26 +319,29 @@ int launch_fused_t(const FusedArgs& a, cudaStream_t s) {
   constexpr size_t smem = FusedSmem<M>::total;
   auto kern = k_fused<M, MODE, LOSS>;
   // the shared-memory attribute and the resident-CTA count are set up once per
-  // device (a per-call host cost otherwise); 0 = not yet known
-  constexpr int kMaxDev = 64;
-  static int slots_cache[kMaxDev] = {};
+  // device (a per-call host cost otherwise)
+  static PtyDevCache slots_cache;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return PTYCHO_ERR_LAUNCH;
-  int slots = slots_cache[dev];
-  if (slots == 0) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-      return PTYCHO_ERR_LAUNCH;
-    int nsm = 148, per_sm = 1;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Plan<M>::NT, smem) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-    slots = nsm * per_sm;
-    slots_cache[dev] = slots;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int slots = slots_cache.get(&dev);
+    if (dev < 0) return PTYCHO_ERR_LAUNCH;
+    if (slots == 0) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return PTYCHO_ERR_LAUNCH;
+      int nsm = 148, per_sm = 1;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Plan<M>::NT, smem) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      slots = nsm * per_sm;
+      slots_cache.put(dev, slots);
+    }
+    const int grid = a.B < slots ? a.B : slots;
+    kern<<<grid, Plan<M>::NT, smem, s>>>(a);
+    if (cudaGetLastError() == cudaSuccess) return PTYCHO_OK;
+    slots_cache.put(dev, 0);  // e.g. the attribute was lost with a device reset: set up again once
   }
-  const int grid = a.B < slots ? a.B : slots;
-  kern<<<grid, Plan<M>::NT, smem, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
+  return PTYCHO_ERR_LAUNCH;
 }
 
 template <int M>

@@ -13,9 +13,14 @@
 //     exits;
 //   * a call whose scratch need (ptycho_fwd_adj_workspace_size) exceeds it is
 //     rejected with PTYCHO_ERR_WORKSPACE before any device work;
-//   * the array's device address is looked up with cudaGetSymbolAddress on the
-//     first call on each device (that device current); make that first call
+//   * the array's device address is looked up with cudaGetSymbolAddress on
+//     every call, in the caller's current context: a __device__ symbol's
+//     address belongs to a CUDA context, so a cached address could point into
+//     memory of a context that was reset or is not current.  The first call in
+//     a context may load the library's module there; make that first call
 //     before any stream capture;
+//   * arguments the workspace entry point would refuse (sizes, probe shape)
+//     are refused with the same status before the address is looked up;
 //   * all calls share the one array and it keeps the last call's contents:
 //     the arrival counters that must start at zero are cleared by the fused
 //     kernel of each call, everything else is written before it is read.
@@ -25,31 +30,19 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <mutex>
-
 #include "../../include/ptycho_b200.h"
 
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(48) << 20;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_scratch_mu;
-void* g_scratch_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
-
-// device address of the scratch array on the current device (looked up once)
-int scratch_for_current_device(void** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PTYCHO_ERR_LAUNCH;
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PTYCHO_ERR_LAUNCH;
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+// device address of the scratch array in the current context
+int scratch_for_current_context(void** out) {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PTYCHO_ERR_LAUNCH;
+  *out = p;
   return PTYCHO_OK;
 }
 
@@ -61,9 +54,13 @@ extern "C" int ptycho_fwd_adj_noalloc(const float* O, int H, int W, const float*
                                       double* loss_per_pattern, double* loss_total, float* dO,
                                       float* dP, unsigned flags, int32_t* status_out,
                                       ptycho_stream_t stream) {
-  if (ptycho_fwd_adj_workspace_size(H, W, M, N, B) > kNoAllocScratchBytes) return PTYCHO_ERR_WORKSPACE;
+  const size_t need = ptycho_fwd_adj_workspace_size(H, W, M, N, B);
+  if (need == 0)  // sizes or probe shape the workspace entry point refuses: its own status, no device work
+    return ptycho_fwd_adj(O, H, W, P, M, N, tl, Imeas, F, batch, B, loss_type, loss_per_pattern,
+                          loss_total, dO, dP, flags, nullptr, 0, status_out, stream);
+  if (need > kNoAllocScratchBytes) return PTYCHO_ERR_WORKSPACE;
   void* scratch = nullptr;
-  const int st = scratch_for_current_device(&scratch);
+  const int st = scratch_for_current_context(&scratch);
   if (st) return st;
   return ptycho_fwd_adj(O, H, W, P, M, N, tl, Imeas, F, batch, B, loss_type, loss_per_pattern,
                         loss_total, dO, dP, flags, scratch, kNoAllocScratchBytes, status_out, stream);

@@ -188,17 +188,22 @@ int ptycho_probe_center_normalize(const float* P, int M, int N, float* P_out, do
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (M * N <= pp::kStageMax) {
     const int smem = M * N * int(sizeof(float2));
-    static bool attr_set[64] = {};  // per device: the dynamic shared-memory limit, once
+    static PtyDevCache attr_set;  // per device: the dynamic shared-memory limit, once
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PTYCHO_ERR_LAUNCH;
-    if (!attr_set[dev]) {
-      if (cudaFuncSetAttribute(pp::k_probe_prep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               pp::kStageMax * int(sizeof(float2))) != cudaSuccess)
-        return PTYCHO_ERR_LAUNCH;
-      attr_set[dev] = true;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      if (!attr_set.get(&dev)) {
+        if (dev < 0) return PTYCHO_ERR_LAUNCH;
+        if (cudaFuncSetAttribute(pp::k_probe_prep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 pp::kStageMax * int(sizeof(float2))) != cudaSuccess)
+          return PTYCHO_ERR_LAUNCH;
+        attr_set.put(dev, 1);
+      }
+      pp::k_probe_prep<true><<<1, pp::NT, smem, s>>>(reinterpret_cast<const float2*>(P), M, N,
+                                                     reinterpret_cast<float2*>(P_out), state);
+      if (cudaGetLastError() == cudaSuccess) return PTYCHO_OK;
+      attr_set.put(dev, 0);  // the attribute was lost (device reset): set it again once
     }
-    pp::k_probe_prep<true><<<1, pp::NT, smem, s>>>(reinterpret_cast<const float2*>(P), M, N,
-                                                   reinterpret_cast<float2*>(P_out), state);
+    return PTYCHO_ERR_LAUNCH;
   } else {
     pp::k_probe_prep<false><<<1, pp::NT, 0, s>>>(reinterpret_cast<const float2*>(P), M, N,
                                                  reinterpret_cast<float2*>(P_out), state);

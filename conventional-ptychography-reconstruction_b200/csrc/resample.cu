@@ -250,9 +250,324 @@ bool supported(int n, int N) {
 }
 
 }  // namespace rs
+
+// ---------------------------------------------------------------------------
+// Any line length (the canvases Recovery.py builds are multiples of 6, so
+// object grids are multiples of 3 and can hold large prime factors: 498 =
+// 2 * 3 * 83).  Per line: forward DFT of length L1, band remap, inverse DFT
+// of length L2, scale -- the same per-axis operator as above, with the remap
+// written for odd lengths too.  With n = min(L1, L2), N = max(L1, L2) and the
+// band k in [lo, lo + n), lo = -floor(n/2), the reference's fftshift /
+// centred pad / ifftshift puts bin k of the length-n spectrum at bin
+// (k + d) mod N of the length-N one, d = floor(n/2) + floor((N-n)/2) -
+// floor(N/2): d = 0 for even n, or odd n and odd N; d = -1 for odd n and even
+// N (the reference's half-bin asymmetry, kept).  The adjoint gathers back.
+//
+// Transforms are Stockham passes with a run-time plan: radix 16, 8, 4, 2, 3,
+// 5, 7 as register butterflies (dft_regs.cuh), any other prime factor p as a
+// direct p-term sum per output with table twiddles.  Passes ping-pong between
+// two shared-memory buffers of float2 (one float2 of padding every 16 breaks
+// the stride-2^k bank conflicts of the first passes).  Twiddles:
+// exp(-2 pi i j / LMAX), LMAX = max(L1, L2) = s * min(L1, L2), rounded from
+// double-precision sincospi; a length-L pass reads it with stride LMAX / L.
+// ---------------------------------------------------------------------------
+namespace rsg {
+
+constexpr int kMaxFactors = 16;
+constexpr int kMaxLen = 8192;
+constexpr int kNT = 512;
+constexpr size_t kSmemCap = 200 * 1024;
+
+struct LinePlan {
+  int L;
+  int nf;
+  int radix[kMaxFactors];
+};
+
+// factor L into passes: powers of two as 16, 8, 4, 2; then 3, 5, 7; any
+// other prime factor gets its own direct-sum pass
+static bool make_plan(int L, LinePlan* p) {
+  if (L < 1 || L > kMaxLen) return false;
+  p->L = L;
+  p->nf = 0;
+  int r = L;
+  auto push = [&](int f) {
+    if (p->nf >= kMaxFactors) return false;
+    p->radix[p->nf++] = f;
+    r /= f;
+    return true;
+  };
+  for (int f : {16, 8, 4, 2})
+    while (r % f == 0)
+      if (!push(f)) return false;
+  for (int f : {3, 5, 7})
+    while (r % f == 0)
+      if (!push(f)) return false;
+  for (int f = 11; r > 1; f += 2)
+    while (r % f == 0)
+      if (!push(f)) return false;
+  return true;
+}
+
+struct Args {
+  const float2* in;
+  float2* out;
+  int nlines;
+  long long ld_in, ld_out;
+  LinePlan f1, f2;  // forward transform (length L1), inverse transform (length L2)
+  int lmax;         // max(L1, L2): twiddle table length
+  int lines;        // lines per CTA
+  int ls;           // padded line stride in float2
+  int d, lo;        // band remap offset and lowest band frequency
+  float scale;
+};
+
+__host__ __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+
+template <int R, bool INV>
+PTY_DEVI void pass_r(const float2* __restrict__ src, float2* __restrict__ dst, const float2* __restrict__ tw,
+                     int L, int NS, int lines, int ls, int lmax, int t) {
+  const int bpl = L / R;
+  const int tws = lmax / (NS * R);
+  for (int b = t; b < lines * bpl; b += kNT) {
+    const int line = b / bpl, j = b - line * bpl;
+    const int k = j % NS;
+    const float2* sl = src + line * ls;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = sl[pad16(j + r * bpl)];
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[k * r * tws];
+        if (INV) w.y = -w.y;
+        v[r] = c_mul(v[r], w);
+      }
+    }
+    dft<R, INV, 1>(v);
+    float2* dl = dst + line * ls;
+    const int o = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dl[pad16(o + r * NS)] = v[r];
+  }
+}
+
+// direct sum for a prime factor p: output o = (j / NS) NS p + k + r NS gets
+// sum_m x[j + m L/p] exp(-+2 pi i m (k + r NS) / (NS p))
+template <bool INV>
+PTY_DEVI void pass_generic(const float2* __restrict__ src, float2* __restrict__ dst, const float2* __restrict__ tw,
+                           int L, int p, int NS, int lines, int ls, int lmax, int t) {
+  const int bpl = L / p;
+  const int blk = NS * p;
+  const int tws = lmax / blk;
+  for (int e = t; e < lines * L; e += kNT) {
+    const int line = e / L, o = e - line * L;
+    const int ob = o / blk, rem = o - ob * blk;
+    const int r = rem / NS, k = rem - r * NS;
+    const int j = ob * NS + k;
+    const int q = (k + r * NS) * tws;  // < lmax
+    const float2* sl = src + line * ls;
+    float2 acc = make_float2(0.f, 0.f);
+    int idx = 0;
+    for (int m = 0; m < p; ++m) {
+      float2 w = tw[idx];
+      if (INV) w.y = -w.y;
+      const float2 x = sl[pad16(j + m * bpl)];
+      acc.x = fmaf(x.x, w.x, fmaf(-x.y, w.y, acc.x));
+      acc.y = fmaf(x.x, w.y, fmaf(x.y, w.x, acc.y));
+      idx += q;
+      if (idx >= lmax) idx -= lmax;
+    }
+    dst[line * ls + pad16(o)] = acc;
+  }
+}
+
+template <bool INV>
+PTY_DEVI void run_pass(int R, const float2* src, float2* dst, const float2* tw, int L, int NS, int lines, int ls,
+                       int lmax, int t) {
+  switch (R) {
+    case 2: pass_r<2, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    case 3: pass_r<3, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    case 4: pass_r<4, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    case 5: pass_r<5, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    case 7: pass_r<7, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    case 8: pass_r<8, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    case 16: pass_r<16, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
+    default: pass_generic<INV>(src, dst, tw, L, R, NS, lines, ls, lmax, t); break;
+  }
+}
+
+// all passes of one plan; returns the buffer that holds the result
+template <bool INV>
+PTY_DEVI float2* transform(const LinePlan& pl, float2* a, float2* b, const float2* tw, int lines, int ls, int lmax,
+                           int t) {
+  int NS = 1;
+  for (int i = 0; i < pl.nf; ++i) {
+    const int R = pl.radix[i];
+    run_pass<INV>(R, a, b, tw, pl.L, NS, lines, ls, lmax, t);
+    __syncthreads();
+    NS *= R;
+    float2* c = a;
+    a = b;
+    b = c;
+  }
+  return a;
+}
+
+template <bool COL>
+__global__ void __launch_bounds__(kNT) k_resample_any(const Args g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lines = g.lines, ls = g.ls, lmax = g.lmax;
+  float2* bufA = reinterpret_cast<float2*>(smem);
+  float2* bufB = bufA + size_t(lines) * ls;
+  float2* tw = bufB + size_t(lines) * ls;
+  const int t = threadIdx.x;
+  const int l0 = blockIdx.x * lines;
+  const int L1 = g.f1.L, L2 = g.f2.L;
+  for (int k = t; k < lmax; k += kNT) {
+    double sn, cs;
+    sincospi(-2.0 * double(k) / double(lmax), &sn, &cs);
+    tw[k] = make_float2(float(cs), float(sn));
+  }
+  for (int idx = t; idx < lines * L1; idx += kNT) {
+    int l, k;
+    if (COL) {
+      l = idx % lines;
+      k = idx / lines;
+    } else {
+      l = idx / L1;
+      k = idx - l * L1;
+    }
+    float2 x = make_float2(0.f, 0.f);
+    if (l0 + l < g.nlines) x = COL ? __ldg(g.in + k * g.ld_in + (l0 + l)) : __ldg(g.in + (l0 + l) * g.ld_in + k);
+    bufA[l * ls + pad16(k)] = x;
+  }
+  __syncthreads();
+  float2* spec = transform<false>(g.f1, bufA, bufB, tw, lines, ls, lmax, t);
+  float2* rem = spec == bufA ? bufB : bufA;
+  // band remap into the other buffer
+  const int n = L1 < L2 ? L1 : L2;
+  for (int idx = t; idx < lines * L2; idx += kNT) {
+    const int l = idx / L2, j = idx - l * L2;
+    float2 v = make_float2(0.f, 0.f);
+    if (L2 >= L1) {  // pad: bin j of the long spectrum holds band frequency k, or nothing
+      int k = (j - g.d - g.lo) % L2;
+      if (k < 0) k += L2;
+      k += g.lo;
+      if (k < g.lo + n) {
+        int src = k % L1;
+        if (src < 0) src += L1;
+        v = spec[l * ls + pad16(src)];
+      }
+    } else {  // crop: bin j of the short spectrum is band frequency k of the long one
+      int k = (j - g.lo) % n;
+      if (k < 0) k += n;
+      k += g.lo;
+      int src = (k + g.d) % L1;
+      if (src < 0) src += L1;
+      v = spec[l * ls + pad16(src)];
+    }
+    rem[l * ls + pad16(j)] = v;
+  }
+  __syncthreads();
+  float2* other = rem == bufA ? bufB : bufA;
+  float2* res = transform<true>(g.f2, rem, other, tw, lines, ls, lmax, t);
+  for (int idx = t; idx < lines * L2; idx += kNT) {
+    int l, k;
+    if (COL) {
+      l = idx % lines;
+      k = idx / lines;
+    } else {
+      l = idx / L2;
+      k = idx - l * L2;
+    }
+    if (l0 + l < g.nlines) {
+      const float2 y = res[l * ls + pad16(k)];
+      const float2 o = make_float2(y.x * g.scale, y.y * g.scale);
+      if (COL)
+        g.out[k * g.ld_out + (l0 + l)] = o;
+      else
+        g.out[(l0 + l) * g.ld_out + k] = o;
+    }
+  }
+}
+
+static size_t smem_bytes(int lines, int ls, int lmax) {
+  return (size_t(2) * lines * ls + size_t(lmax)) * sizeof(float2);
+}
+
+// true when the pair of line lengths is handled (one a whole multiple of the other)
+static bool supported_pair(int l1, int l2) {
+  if (l1 < 1 || l2 < 1 || l1 > kMaxLen || l2 > kMaxLen) return false;
+  const int lo = l1 < l2 ? l1 : l2, hi = l1 < l2 ? l2 : l1;
+  return hi % lo == 0;
+}
+
+// lines of length l1 -> lines of length l2: forward DFT, band remap, inverse DFT, scale 1 / min(l1, l2)
+template <bool COL>
+static int launch(int l1, int l2, const float2* in, float2* out, int nlines, long long ld_in, long long ld_out,
+                  cudaStream_t s) {
+  if (!supported_pair(l1, l2)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  Args g{};
+  if (!make_plan(l1, &g.f1) || !make_plan(l2, &g.f2)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  g.in = in;
+  g.out = out;
+  g.nlines = nlines;
+  g.ld_in = ld_in;
+  g.ld_out = ld_out;
+  const int n = l1 < l2 ? l1 : l2, N = l1 < l2 ? l2 : l1;
+  g.lmax = N;
+  g.lo = -(n / 2);
+  g.d = n / 2 + (N - n) / 2 - N / 2;
+  g.scale = 1.0f / float(n);
+  g.ls = pad16(N - 1) + 1;
+  // lines per CTA: ~8192 values, at least 4 adjacent columns (32-byte
+  // segments) in the column pass, within the shared-memory cap
+  int lines = N >= 8192 ? 1 : 8192 / N;
+  if (COL && lines < 4) lines = 4;
+  while (lines > 1 && smem_bytes(lines, g.ls, N) > kSmemCap) --lines;
+  g.lines = lines;
+  const size_t smem = smem_bytes(lines, g.ls, N);
+  auto kern = k_resample_any<COL>;
+  static PtyDevCache attr_set;
+  int dev = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    if (!attr_set.get(&dev)) {
+      if (dev < 0) return PTYCHO_ERR_LAUNCH;
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemCap)) != cudaSuccess)
+        return PTYCHO_ERR_LAUNCH;
+      attr_set.put(dev, 1);
+    }
+    kern<<<(nlines + lines - 1) / lines, kNT, smem, s>>>(g);
+    if (cudaGetLastError() == cudaSuccess) return PTYCHO_OK;
+    attr_set.put(dev, 0);
+  }
+  return PTYCHO_ERR_LAUNCH;
+}
+
+}  // namespace rsg
 }  // namespace pty
 
 using namespace pty;
+
+namespace {
+
+// power-of-two pairs keep the compile-time kernels; every other pair runs the
+// run-time-planned one
+template <bool COL>
+int line_pass(int l1, int l2, const float2* in, float2* out, int nlines, long long ld_in, long long ld_out,
+              cudaStream_t s) {
+  if (rs::supported(l1, l2)) return rs::dispatch<COL>(l1, l2, in, out, nlines, ld_in, ld_out, s);
+  return rsg::launch<COL>(l1, l2, in, out, nlines, ld_in, ld_out, s);
+}
+
+bool supported_upsample(int h, int w, int s) {
+  if (h <= 0 || w <= 0 || s <= 0) return false;
+  if (h > rsg::kMaxLen / s || w > rsg::kMaxLen / s) return false;
+  return true;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -264,31 +579,31 @@ size_t ptycho_fourier_upsample_workspace_size(int h, int w, int s) {
 int ptycho_fourier_upsample(const float* x, int h, int w, int s, float* y, void* workspace,
                             size_t workspace_bytes, ptycho_stream_t stream) {
   if (!x || !y || h <= 0 || w <= 0 || s <= 0) return PTYCHO_ERR_INVALID_ARG;
-  if (!rs::supported(h, h * s) || !rs::supported(w, w * s)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  if (!supported_upsample(h, w, s)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
   if (!workspace || workspace_bytes < ptycho_fourier_upsample_workspace_size(h, w, s))
     return PTYCHO_ERR_WORKSPACE;
   if (!pty_aligned(x, 8) || !pty_aligned(y, 8) || !pty_aligned(workspace, 8)) return PTYCHO_ERR_MISALIGNED;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int W = w * s, H = h * s;
   float2* tmp = static_cast<float2*>(workspace);
-  int rc = rs::dispatch<false>(w, W, reinterpret_cast<const float2*>(x), tmp, h, w, W, st);  // rows
+  int rc = line_pass<false>(w, W, reinterpret_cast<const float2*>(x), tmp, h, w, W, st);  // rows
   if (rc) return rc;
-  return rs::dispatch<true>(h, H, tmp, reinterpret_cast<float2*>(y), W, W, W, st);           // columns
+  return line_pass<true>(h, H, tmp, reinterpret_cast<float2*>(y), W, W, W, st);           // columns
 }
 
 int ptycho_fourier_upsample_adjoint(const float* gy, int h, int w, int s, float* gx, void* workspace,
                                     size_t workspace_bytes, ptycho_stream_t stream) {
   if (!gy || !gx || h <= 0 || w <= 0 || s <= 0) return PTYCHO_ERR_INVALID_ARG;
-  if (!rs::supported(h, h * s) || !rs::supported(w, w * s)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  if (!supported_upsample(h, w, s)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
   if (!workspace || workspace_bytes < ptycho_fourier_upsample_workspace_size(h, w, s))
     return PTYCHO_ERR_WORKSPACE;
   if (!pty_aligned(gy, 8) || !pty_aligned(gx, 8) || !pty_aligned(workspace, 8)) return PTYCHO_ERR_MISALIGNED;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int W = w * s, H = h * s;
   float2* tmp = static_cast<float2*>(workspace);  // [H][w]
-  int rc = rs::dispatch<false>(W, w, reinterpret_cast<const float2*>(gy), tmp, H, W, w, st);  // rows
+  int rc = line_pass<false>(W, w, reinterpret_cast<const float2*>(gy), tmp, H, W, w, st);  // rows
   if (rc) return rc;
-  return rs::dispatch<true>(H, h, tmp, reinterpret_cast<float2*>(gx), w, w, w, st);           // columns
+  return line_pass<true>(H, h, tmp, reinterpret_cast<float2*>(gx), w, w, w, st);           // columns
 }
 
 }  // extern "C"

@@ -5,8 +5,11 @@ models/complex_inr.py:252-271 computes with torch.fft:
 ``ifft2(ifftshift(pad(fftshift(fft2(x))))) * s**2`` -> [h*s, w*s], with the
 backward pass (the operator's conjugate transpose) on the same kernels
 (``ptycho_fourier_upsample`` / ``ptycho_fourier_upsample_adjoint``).
-Sizes: h, w, h*s, w*s powers of two in [64, 4096], s in {1, 2, 4}
-(``supported``); callers keep the torch.fft formula for other shapes.
+Sizes: any h, w >= 1 and integer s >= 1 with h*s, w*s <= 8192 (``supported``).
+Power-of-two lines run compile-time radix-8/16 kernels; every other length
+(the multiples of 3 that Recovery.py's canvases give, odd lengths, large
+prime factors) runs the run-time-planned mixed-radix kernel.  There is no
+torch.fft path: other shapes raise.
 """
 from __future__ import annotations
 
@@ -14,16 +17,14 @@ import torch
 
 from . import _lib
 
-
-def _pow2(n: int) -> bool:
-    return 64 <= n <= 4096 and n & (n - 1) == 0
+MAX_LEN = 8192
 
 
 def supported(h: int, w: int, s) -> bool:
-    if int(s) != s or int(s) not in (1, 2, 4):
+    if int(s) != s or int(s) < 1:
         return False
     s = int(s)
-    return _pow2(h) and _pow2(w) and _pow2(h * s) and _pow2(w * s)
+    return 1 <= h and 1 <= w and h * s <= MAX_LEN and w * s <= MAX_LEN
 
 
 def _workspace(h, w, s, dev):

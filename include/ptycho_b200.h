@@ -379,9 +379,12 @@ int ptycho_gs_backward(int kind, const float* xy, const float* p1, const float* 
  * library, held by every GPU that loads it until the process exits.  A call
  * needing more than 48 MiB of scratch (ptycho_fwd_adj_workspace_size) returns
  * PTYCHO_ERR_WORKSPACE without touching the device (M = 128 fits up to about
- * 360 patterns per call).  The first call on a device looks up the array's
- * address; make it before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race, so order them on one stream.
+ * 360 patterns per call).  Arguments ptycho_fwd_adj refuses get its status
+ * first, before any lookup.  Every call looks up the array's address in the
+ * current context (an address cached from another context could be stale);
+ * the first call in a context may load the module, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race, so order them on one stream.
  * ---------------------------------------------------------------------- */
 int ptycho_fwd_adj_noalloc(const float* O, int H, int W, const float* P, int M, int N,
                            const int32_t* tl, const float* Imeas, int F, const int32_t* batch,

@@ -1,6 +1,7 @@
 """Build oracle/_ref/libgscp_ref.so: the reference's own Gaussian rasteriser
 (gscp/csrc/gscp_rasterizer/{forward,backward,rasterizer_impl}.cu, compiled
-from the sources where they lie under /root/reference, with the reference's
+from the sources where they lie in the reference tree (``PTYCHO_REFERENCE``,
+default /root/reference), with the reference's
 nvcc flags -O3 --use_fast_math, gscp/csrc/setup.py:25-27) plus the C entry
 points of oracle/gscp_ref_shim.cu.  TEST ONLY: the parity tests load it as a
 checker.  Skipped (returns None) when the reference tree or nvcc is absent,
@@ -15,7 +16,8 @@ import shutil
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/gscp/csrc/gscp_rasterizer"
+REF_ROOT = os.environ.get("PTYCHO_REFERENCE", "/root/reference")
+REF = os.path.join(REF_ROOT, "gscp", "csrc", "gscp_rasterizer")
 OUT = os.path.join(HERE, "_ref", "libgscp_ref.so")
 SOURCES = ["forward.cu", "backward.cu", "rasterizer_impl.cu"]
 

@@ -72,8 +72,9 @@ def test_fourier_upsample_validation_before_device_work():
     n = L.ptycho_fourier_upsample_workspace_size(512, 512, 2)
     assert n == 512 * 512 * 2 * 8 and L.ptycho_fourier_upsample_workspace_size(0, 8, 2) == 0
     for fn in (L.ptycho_fourier_upsample, L.ptycho_fourier_upsample_adjoint):
-        assert fn(fake, 96, 96, 2, fake, fake, n, None) == st["UNSUPPORTED_SIZE"]
-        assert fn(fake, 64, 64, 8, fake, fake, n, None) == st["UNSUPPORTED_SIZE"]
+        assert fn(fake, 4097, 96, 2, fake, fake, n, None) == st["UNSUPPORTED_SIZE"]  # line > 8192
+        assert fn(fake, 64, 2048, 8, fake, fake, n, None) == st["UNSUPPORTED_SIZE"]
+        assert fn(fake, 96, 96, 0, fake, fake, n, None) == st["INVALID_ARG"]
         assert fn(None, 64, 64, 2, fake, fake, n, None) == st["INVALID_ARG"]
         assert fn(fake, 512, 512, 2, fake, fake, n - 8, None) == st["WORKSPACE"]
         assert fn(ctypes.c_void_p(4100), 512, 512, 2, fake, fake, n, None) == st["MISALIGNED"]

@@ -35,7 +35,7 @@ def test_reference_configs_parse():
     import os
     import glob
     from conftest import ROOT
-    ref = "/root/reference/config"
+    ref = os.path.join(os.environ.get("PTYCHO_REFERENCE", "/root/reference"), "config")
     if not os.path.isdir(ref):
         pytest.skip("reference tree not present")
     for f in glob.glob(os.path.join(ref, "*.yaml")):
