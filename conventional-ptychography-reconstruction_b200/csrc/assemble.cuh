@@ -12,11 +12,11 @@ constexpr int kPixBlock = 256;  // probe pixels per dP block
 inline int dp_counters(int M) { return (M * M + kPixBlock - 1) / kPixBlock; }
 
 // dP (group partials, then the last-arriving block sums them in group order),
-// dO (tile owner sums in ascending pattern order) and the FP64 loss total; any
-// output may be null.  E' is overwritten (with the object-gradient terms) when
-// dO is requested.  `done` holds dp_counters(M) zeroed counters.
-int launch_assemble(float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W, int M,
-                    float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
+// dO (tile owner sums in ascending pattern order) and the FP64 loss total in
+// one launch; any output may be null.  E' is only read.  `done` holds
+// dp_counters(M) zeroed counters and is left zeroed.
+int launch_assemble(const float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W,
+                    int M, float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
                     double* loss_total, bool accumulate, cudaStream_t s);
 
 }  // namespace pty
