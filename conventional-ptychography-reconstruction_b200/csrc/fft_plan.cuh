@@ -173,6 +173,17 @@ PTY_DEVI void static_for(Fn&& f) {
 // ---------------------------------------------------------------------------
 // one DIF pass (forward) or its adjoint, on the register array v
 // ---------------------------------------------------------------------------
+// twiddle table entry i, read with a volatile shared-memory load: the loads
+// are issued where they are used instead of all being hoisted ahead of the
+// butterflies, which keeps the 32-value passes inside the register budget
+PTY_DEVI float2 tw_load(const float2* __restrict__ tw, int i) {
+  float2 w;
+  asm volatile("ld.volatile.shared.v2.f32 {%0, %1}, [%2];"
+               : "=f"(w.x), "=f"(w.y)
+               : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(tw + i))));
+  return w;
+}
+
 template <int M, int E, bool ADJ, int RX, int RY, int LOX, int NBX, int LOY, int NBY>
 PTY_DEVI void run_pass(float2 (&v)[E], int bx, int by, const float2* __restrict__ tw) {
   constexpr int LOGM = Plan<M>::LOGM;
@@ -184,19 +195,29 @@ PTY_DEVI void run_pass(float2 (&v)[E], int bx, int by, const float2* __restrict_
     if constexpr (!ADJ) {
 #pragma unroll
       for (int j = 0; j < RY * REP; ++j) dft<RX, false, 1>(v + RX * j);
-    }
-    if constexpr (LOX > 0) {
+      if constexpr (LOX > 0) {
 #pragma unroll
-      for (int k = 1; k < RX; ++k) {
-        float2 w = tw[((n2 * k) << SH) & (M - 1)];
-        if constexpr (ADJ) w.y = -w.y;
+        for (int k = 1; k < RX; ++k) {
+          const float2 w = tw[((n2 * k) << SH) & (M - 1)];
 #pragma unroll
-        for (int j = 0; j < RY * REP; ++j) v[k + RX * j] = c_mul(v[k + RX * j], w);
+          for (int j = 0; j < RY * REP; ++j) v[k + RX * j] = c_mul(v[k + RX * j], w);
+        }
       }
-    }
-    if constexpr (ADJ) {
+    } else {
+      // one line at a time: conjugate twiddles (volatile loads, issued where
+      // they are used), then the inverse DFT
 #pragma unroll
-      for (int j = 0; j < RY * REP; ++j) dft<RX, true, 1>(v + RX * j);
+      for (int j = 0; j < RY * REP; ++j) {
+        if constexpr (LOX > 0) {
+#pragma unroll
+          for (int k = 1; k < RX; ++k) {
+            float2 w = tw_load(tw, ((n2 * k) << SH) & (M - 1));
+            w.y = -w.y;
+            v[k + RX * j] = c_mul(v[k + RX * j], w);
+          }
+        }
+        dft<RX, true, 1>(v + RX * j);
+      }
     }
   }
   if constexpr (RY > 1) {
