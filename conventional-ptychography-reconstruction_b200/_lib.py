@@ -24,6 +24,9 @@ SIGNATURES = {
     "ptycho_version": (_c_int, []),
     "ptycho_forward_intensity": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp,
                                           _c_int, _vp, _vp, _vp]),
+    "ptycho_forward_intensity_workspace_size": (_c_size, [_c_int, _c_int, _c_int]),
+    "ptycho_forward_intensity_ws": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp,
+                                             _c_int, _vp, _vp, _c_size, _vp, _vp]),
     "ptycho_fwd_adj_workspace_size": (_c_size, [_c_int, _c_int, _c_int, _c_int, _c_int]),
     "ptycho_fwd_adj": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _c_int,
                                 _c_int, _vp, _vp, _vp, _vp, _c_uint, _vp, _c_size, _vp, _vp]),

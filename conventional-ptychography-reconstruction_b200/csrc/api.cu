@@ -4,39 +4,46 @@
 
 #include "assemble.cuh"
 #include "fused.cuh"
+#include "general.cuh"
 
 namespace pty {
 
 struct WsLayout {
-  size_t E, part, loss, tlb, done, total;
+  size_t E, scr, part, loss, tlb, done, total;
 };
 
-static WsLayout ws_layout(int M, int B) {
+// square 64, 128, 256: the fused kernels; every other M x N: the general path
+static bool fused_probe(int M, int N) { return M == N && (M == 64 || M == 128 || M == 256); }
+
+static WsLayout ws_layout(int M, int N, int B) {
   const size_t G = (size_t(B) + kGroup - 1) / kGroup;
+  const size_t MN = size_t(M) * N;
   WsLayout L;
   size_t off = 0;
   L.E = off;
-  off += pty_align_up(size_t(B) * M * M * sizeof(float2), 256);
+  off += pty_align_up(size_t(B) * MN * sizeof(float2), 256);
+  L.scr = off;  // the general path's FD planes
+  if (!fused_probe(M, N)) off += pty_align_up(size_t(B) * MN * 3 * sizeof(float), 256);
   L.part = off;
-  off += pty_align_up(G * M * M * sizeof(float2), 256);
+  off += pty_align_up(G * MN * sizeof(float2), 256);
   L.loss = off;
   off += pty_align_up(size_t(B) * sizeof(double), 256);
   L.tlb = off;
   off += pty_align_up(size_t(B) * sizeof(int2), 256);
   L.done = off;  // arrival counters of the dP reduction (self-resetting)
-  off += pty_align_up(size_t(dp_counters(M)) * sizeof(unsigned), 256);
+  off += pty_align_up(size_t(dp_counters(M, N)) * sizeof(unsigned), 256);
   L.total = off;
   return L;
 }
 
-static bool supported_probe(int M, int N) { return M == N && (M == 64 || M == 128 || M == 256); }
+static bool supported_probe(int M, int N) { return fused_probe(M, N) || general_supported(M, N); }
 
 static int check_common(const float* O, int H, int W, const float* P, int M, int N, const int32_t* tl,
                         int F, const int32_t* batch, int B) {
   if (!O || !P || (B > 0 && !tl) || H <= 0 || W <= 0 || B < 0 || F < 0) return PTYCHO_ERR_INVALID_ARG;
   if (!batch && B > F) return PTYCHO_ERR_INVALID_ARG;
   if (!supported_probe(M, N)) return PTYCHO_ERR_UNSUPPORTED_SIZE;
-  if (H < M || W < M) return PTYCHO_ERR_INVALID_ARG;
+  if (H < M || W < N) return PTYCHO_ERR_INVALID_ARG;
   if (!pty_aligned(O, 8) || !pty_aligned(P, 8) || !pty_aligned(tl, 8) || !pty_aligned(batch, 4))
     return PTYCHO_ERR_MISALIGNED;
   return PTYCHO_OK;
@@ -96,12 +103,37 @@ int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   FusedArgs a = make_args(O, H, W, P, tl, nullptr, F, batch, B, status_out);
   a.I_out = I_out;
-  return launch_fused(M, MODE_INTENSITY, 0, a, s);
+  if (fused_probe(M, N)) return launch_fused(M, MODE_INTENSITY, 0, a, s);
+  return PTYCHO_ERR_UNSUPPORTED_SIZE;  // other shapes need scratch: ptycho_forward_intensity_ws
+}
+
+size_t ptycho_forward_intensity_workspace_size(int M, int N, int B) {
+  if (B < 0 || !supported_probe(M, N)) return 0;
+  if (fused_probe(M, N)) return 256;  // the fused kernels need none
+  return pty_align_up(size_t(B) * M * N * sizeof(float2), 256);
+}
+
+int ptycho_forward_intensity_ws(const float* O, int H, int W, const float* P, int M, int N,
+                                const int32_t* tl, int F, const int32_t* batch, int B, float* I_out,
+                                void* workspace, size_t workspace_bytes, int32_t* status_out,
+                                ptycho_stream_t stream) {
+  int st = check_common(O, H, W, P, M, N, tl, F, batch, B);
+  if (st) return st;
+  if (B == 0) return PTYCHO_OK;
+  if (!I_out) return PTYCHO_ERR_INVALID_ARG;
+  if (fused_probe(M, N))
+    return ptycho_forward_intensity(O, H, W, P, M, N, tl, F, batch, B, I_out, status_out, stream);
+  if (!workspace || workspace_bytes < ptycho_forward_intensity_workspace_size(M, N, B)) return PTYCHO_ERR_WORKSPACE;
+  if (!pty_aligned(workspace, 256)) return PTYCHO_ERR_MISALIGNED;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  FusedArgs a = make_args(O, H, W, P, tl, nullptr, F, batch, B, status_out);
+  a.I_out = I_out;
+  return general_forward_intensity(a, M, N, static_cast<float2*>(workspace), s);
 }
 
 size_t ptycho_fwd_adj_workspace_size(int H, int W, int M, int N, int B) {
   if (H <= 0 || W <= 0 || B < 0 || !supported_probe(M, N)) return 0;
-  return ws_layout(M, B).total;
+  return ws_layout(M, N, B).total;
 }
 
 int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, const int32_t* tl,
@@ -115,7 +147,7 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   if (B > 0 && !Imeas) return PTYCHO_ERR_INVALID_ARG;
   if (!pty_aligned(Imeas, 16)) return PTYCHO_ERR_MISALIGNED;
   if ((dO && !pty_aligned(dO, 8)) || (dP && !pty_aligned(dP, 8))) return PTYCHO_ERR_MISALIGNED;
-  const WsLayout L = ws_layout(M, B);
+  const WsLayout L = ws_layout(M, N, B);
   if (!workspace || workspace_bytes < L.total) return PTYCHO_ERR_WORKSPACE;
   if (!pty_aligned(workspace, 256)) return PTYCHO_ERR_MISALIGNED;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -130,7 +162,7 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   if (B == 0) {  // empty batch: zero gradients and loss
     if (!acc) {
       if (dO) cudaMemsetAsync(dO, 0, size_t(H) * W * sizeof(float2), s);
-      if (dP) cudaMemsetAsync(dP, 0, size_t(M) * M * sizeof(float2), s);
+      if (dP) cudaMemsetAsync(dP, 0, size_t(M) * N * sizeof(float2), s);
     }
     if (loss_total) cudaMemsetAsync(loss_total, 0, sizeof(double), s);
     return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
@@ -138,17 +170,25 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   FusedArgs a = make_args(O, H, W, P, tl, Imeas, F, batch, B, status_out);
   a.loss_pat = lp;
   const bool adj = dO || dP;
-  if (adj) {
-    a.Eout = Ews;
-    a.tlb = tlb;
-    a.done = done;
-    a.ndone = dp_counters(M);
+  const bool fused = fused_probe(M, N);
+  if (fused) {
+    if (adj) {
+      a.Eout = Ews;
+      a.tlb = tlb;
+      a.done = done;
+      a.ndone = dp_counters(M, N);
+    }
+    st = launch_fused(M, adj ? MODE_ADJ : MODE_LOSS, loss_type, a, s);
+  } else {
+    // the arrival counters start at zero: the fused kernel zeroes them, here a memset
+    if (adj && cudaMemsetAsync(done, 0, size_t(dp_counters(M, N)) * sizeof(unsigned), s) != cudaSuccess)
+      return PTYCHO_ERR_LAUNCH;
+    st = general_fwd_adj(a, M, N, loss_type, adj, Ews, reinterpret_cast<float*>(ws + L.scr), tlb, s);
   }
-  st = launch_fused(M, adj ? MODE_ADJ : MODE_LOSS, loss_type, a, s);
   if (st) return st;
-  return launch_assemble(Ews, reinterpret_cast<const float2*>(O), reinterpret_cast<const float2*>(P),
-                         tlb, B, H, W, M, reinterpret_cast<float2*>(dO), reinterpret_cast<float2*>(dP),
-                         part, done, lp, loss_total, acc, s);
+  return launch_assemble(Ews, reinterpret_cast<const float2*>(O), reinterpret_cast<const float2*>(P), tlb, B, H,
+                         W, M, N, fused, reinterpret_cast<float2*>(dO), reinterpret_cast<float2*>(dP), part, done,
+                         lp, loss_total, acc, s);
 }
 
 }  // extern "C"

@@ -16,6 +16,9 @@
 //     The sign (-1)^(lx+ly) of a local pixel splits into (-1)^(X+Y) of the
 //     canvas pixel, applied once to the sum, and (-1)^(tlY+tlX) of the
 //     pattern, uniform over the tile.
+// Windows are M x N.  The fused kernels fold fftshift into E' as (-1)^(x+y)
+// (SIGNED); the general path's E is dL/dpsi itself.  dP blocks take two
+// adjacent pixels per thread (16-byte loads) when N is even, else one.
 // No floating-point atomics: every output element is owned by one thread that
 // sums its contributions in a fixed order, so results are bitwise deterministic.
 #include "assemble.cuh"
@@ -59,7 +62,7 @@ struct AsmArgs {
   const float2* O;
   const float2* P;
   const int2* tlb;
-  int B, H, W, M;
+  int B, H, W, M, N;  // windows are M x N
   float2* dO;
   float2* dP;
   float2* part;
@@ -71,43 +74,51 @@ struct AsmArgs {
   int ntx;      // dO tiles per canvas row
 };
 
-// dP role: block (p, g), two adjacent probe pixels per thread (16-byte E'
-// loads), four patterns' loads in flight
+// dP role: block (p, g), PAIR = 2 adjacent probe pixels per thread (16-byte
+// E' loads; N even) or 1, four patterns' loads in flight
+template <bool SIGNED, int PAIR>
 PTY_DEVI void dp_block(const AsmArgs& a, int p, int g) {
   __shared__ int last;
-  const int M = a.M;
-  const size_t MM = size_t(M) * M;
-  const int idx = 2 * (p * kPixBlock + threadIdx.x);  // even: the pair (x, x + 1) shares a row
-  const bool in = idx < M * M;
-  const int y = idx / M, x = idx - (idx / M) * M;
+  const int N = a.N;
+  const size_t MN = size_t(a.M) * N;
+  const int idx = PAIR * (p * kPixBlock + threadIdx.x);  // PAIR 2: (x, x + 1) share a row
+  const bool in = idx < int(MN);
+  const int y = idx / N, x = idx - (idx / N) * N;
   if (in) {
-    const int odd = (x + y) & 1;
+    const int odd = SIGNED ? (x + y) & 1 : 0;
     float2 acc0 = make_float2(0.f, 0.f), acc1 = make_float2(0.f, 0.f);
     const int b1 = min(a.B, (g + 1) * kGroup);
     constexpr int U = 4;
     for (int b = g * kGroup; b < b1; b += U) {
-      float4 e[U];
-      float2 o0[U], o1[U];
+      float2 e0[U], e1[U], o0[U], o1[U];
 #pragma unroll
       for (int k = 0; k < U; ++k) {
         const int2 c = b + k < b1 ? __ldg(a.tlb + b + k) : make_int2(-1, -1);
-        e[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        o0[k] = o1[k] = make_float2(0.f, 0.f);
+        e0[k] = e1[k] = o0[k] = o1[k] = make_float2(0.f, 0.f);
         if (c.x >= 0) {
-          e[k] = __ldg(reinterpret_cast<const float4*>(a.Eb + size_t(b + k) * MM + idx));
           const float2* o = a.O + size_t(c.x + y) * a.W + c.y + x;
+          if constexpr (PAIR == 2) {
+            const float4 e = __ldg(reinterpret_cast<const float4*>(a.Eb + size_t(b + k) * MN + idx));
+            e0[k] = make_float2(e.x, e.y);
+            e1[k] = make_float2(e.z, e.w);
+            o1[k] = __ldg(o + 1);
+          } else {
+            e0[k] = __ldg(a.Eb + size_t(b + k) * MN + idx);
+          }
           o0[k] = __ldg(o);
-          o1[k] = __ldg(o + 1);
         }
       }
 #pragma unroll
       for (int k = 0; k < U; ++k) {  // ascending pattern order
-        c_fma_conj(acc0, make_float2(e[k].x, e[k].y), o0[k]);
-        c_fma_conj(acc1, make_float2(e[k].z, e[k].w), o1[k]);
+        c_fma_conj(acc0, e0[k], o0[k]);
+        if constexpr (PAIR == 2) c_fma_conj(acc1, e1[k], o1[k]);
       }
     }
-    const float2 r0 = c_negif(acc0, odd), r1 = c_negif(acc1, odd ^ 1);
-    __stcg(reinterpret_cast<float4*>(a.part + size_t(g) * MM + idx), make_float4(r0.x, r0.y, r1.x, r1.y));
+    const float2 r0 = c_negif(acc0, odd), r1 = c_negif(acc1, odd ^ int(SIGNED));
+    if constexpr (PAIR == 2)
+      __stcg(reinterpret_cast<float4*>(a.part + size_t(g) * MN + idx), make_float4(r0.x, r0.y, r1.x, r1.y));
+    else
+      __stcg(a.part + size_t(g) * MN + idx, r0);
   }
   __threadfence();
   __syncthreads();
@@ -118,28 +129,33 @@ PTY_DEVI void dp_block(const AsmArgs& a, int p, int g) {
     if (in) {
       float2 r0 = make_float2(0.f, 0.f), r1 = make_float2(0.f, 0.f);
       for (int gg = 0; gg < a.ng; ++gg) {
-        const float4 v = __ldcg(reinterpret_cast<const float4*>(a.part + size_t(gg) * MM + idx));
-        r0 = c_add(r0, make_float2(v.x, v.y));
-        r1 = c_add(r1, make_float2(v.z, v.w));
+        if constexpr (PAIR == 2) {
+          const float4 v = __ldcg(reinterpret_cast<const float4*>(a.part + size_t(gg) * MN + idx));
+          r0 = c_add(r0, make_float2(v.x, v.y));
+          r1 = c_add(r1, make_float2(v.z, v.w));
+        } else {
+          r0 = c_add(r0, __ldcg(a.part + size_t(gg) * MN + idx));
+        }
       }
       if (a.accumulate) {
         r0 = c_add(a.dP[idx], r0);
-        r1 = c_add(a.dP[idx + 1], r1);
+        if constexpr (PAIR == 2) r1 = c_add(a.dP[idx + 1], r1);
       }
       a.dP[idx] = r0;
-      a.dP[idx + 1] = r1;
+      if constexpr (PAIR == 2) a.dP[idx + 1] = r1;
     }
     if (threadIdx.x == 0) a.done[p] = 0u;  // ready for the next call
   }
 }
 
 // dO role: one kTile x kTile canvas tile; lane = column, warp w = rows w + 8 j
+template <bool SIGNED>
 PTY_DEVI void do_block(const AsmArgs& a, int tile) {
   __shared__ int lb[256];
   __shared__ int2 lc[256];
   __shared__ int wcnt[8];
-  const int M = a.M;
-  const size_t MM = size_t(M) * M;
+  const int M = a.M, N = a.N;
+  const size_t MN = size_t(M) * N;
   const int ty0 = (tile / a.ntx) * kTile, tx0 = (tile % a.ntx) * kTile;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int X = tx0 + lane;
@@ -154,7 +170,7 @@ PTY_DEVI void do_block(const AsmArgs& a, int tile) {
     int2 c = make_int2(-1, -1);
     if (b < a.B) {
       c = __ldg(a.tlb + b);
-      hit = c.x >= 0 && c.x < ty0 + kTile && c.x + M > ty0 && c.y < tx0 + kTile && c.y + M > tx0;
+      hit = c.x >= 0 && c.x < ty0 + kTile && c.x + M > ty0 && c.y < tx0 + kTile && c.y + N > tx0;
     }
     const unsigned m = __ballot_sync(0xffffffffu, hit);
     if (lane == 0) wcnt[w] = __popc(m);
@@ -174,16 +190,16 @@ PTY_DEVI void do_block(const AsmArgs& a, int tile) {
     for (int i = 0; i < n; ++i) {
       const int bb = lb[i];
       const int2 cc = lc[i];
-      const unsigned sg = unsigned((cc.x + cc.y) & 1) << 31;  // (-1)^(tlY + tlX) of the pattern
+      const unsigned sg = SIGNED ? unsigned((cc.x + cc.y) & 1) << 31 : 0u;  // (-1)^(tlY + tlX) of the pattern
       const int lx = X - cc.y;
       const int ly0 = Y0 - cc.x;
-      const float2* Eg = a.Eb + size_t(bb) * MM;
+      const float2* Eg = a.Eb + size_t(bb) * MN;
       float2 e[R], p[R];
-      const bool full = cc.x <= ty0 && cc.x + M >= ty0 + kTile && cc.y <= tx0 && cc.y + M >= tx0 + kTile;
+      const bool full = cc.x <= ty0 && cc.x + M >= ty0 + kTile && cc.y <= tx0 && cc.y + N >= tx0 + kTile;
       if (full) {  // uniform: the window covers the whole tile
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-          const int o = (ly0 + 8 * j) * M + lx;
+          const int o = (ly0 + 8 * j) * N + lx;
           e[j] = __ldg(Eg + o);
           p[j] = __ldg(a.P + o);
         }
@@ -192,9 +208,9 @@ PTY_DEVI void do_block(const AsmArgs& a, int tile) {
         for (int j = 0; j < R; ++j) {
           const int ly = ly0 + 8 * j;
           e[j] = p[j] = make_float2(0.f, 0.f);
-          if (lx >= 0 && lx < M && ly >= 0 && ly < M) {
-            e[j] = __ldg(Eg + ly * M + lx);
-            p[j] = __ldg(a.P + ly * M + lx);
+          if (lx >= 0 && lx < N && ly >= 0 && ly < M) {
+            e[j] = __ldg(Eg + ly * N + lx);
+            p[j] = __ldg(a.P + ly * N + lx);
           }
         }
       }
@@ -207,7 +223,7 @@ PTY_DEVI void do_block(const AsmArgs& a, int tile) {
   for (int j = 0; j < R; ++j) {
     const int Y = Y0 + 8 * j;
     if (Y < a.H && X < a.W) {
-      const float2 v = c_negif(acc[j], (X + Y) & 1);
+      const float2 v = SIGNED ? c_negif(acc[j], (X + Y) & 1) : acc[j];
       float2* o = a.dO + size_t(Y) * a.W + X;
       *o = a.accumulate ? c_add(*o, v) : v;
     }
@@ -215,28 +231,30 @@ PTY_DEVI void do_block(const AsmArgs& a, int tile) {
 }
 
 // blocks [0, np * ng): dP role; the rest: dO tiles
+template <bool SIGNED, int PAIR>
 __global__ void __launch_bounds__(256) k_assemble(const AsmArgs a) {
   const int bid = blockIdx.x;
   const int ndp = a.np * a.ng;
   if (bid < ndp) {
     const int p = bid % a.np, g = bid / a.np;
-    dp_block(a, p, g);
+    dp_block<SIGNED, PAIR>(a, p, g);
     if (p == 0 && g == 0 && a.loss_total) {
       __syncthreads();
       loss_sum_block(a.loss_pat, a.B, a.loss_total);
     }
   } else {
-    do_block(a, bid - ndp);
+    do_block<SIGNED>(a, bid - ndp);
   }
 }
 
 int launch_assemble(const float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W,
-                    int M, float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
-                    double* loss_total, bool accumulate, cudaStream_t s) {
+                    int M, int N, bool fftshift_sign, float2* dO, float2* dP, float2* part, unsigned* done,
+                    const double* loss_pat, double* loss_total, bool accumulate, cudaStream_t s) {
   if (!dO && !dP) {
     if (loss_total) k_loss_total<<<1, 256, 0, s>>>(loss_pat, B, loss_total);
     return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
   }
+  const int pair = N % 2 == 0 ? 2 : 1;
   AsmArgs a{};
   a.Eb = Eb;
   a.O = O;
@@ -246,6 +264,7 @@ int launch_assemble(const float2* Eb, const float2* O, const float2* P, const in
   a.H = H;
   a.W = W;
   a.M = M;
+  a.N = N;
   a.dO = dO;
   a.dP = dP;
   a.part = part;
@@ -253,13 +272,18 @@ int launch_assemble(const float2* Eb, const float2* O, const float2* P, const in
   a.loss_pat = loss_pat;
   a.loss_total = loss_total;
   a.accumulate = accumulate ? 1 : 0;
-  a.np = dP ? (M * M / 2 + kPixBlock - 1) / kPixBlock : 0;
+  a.np = dP ? (M * N / pair + kPixBlock - 1) / kPixBlock : 0;
   a.ng = dP ? (B + kGroup - 1) / kGroup : 0;
   a.ntx = (W + kTile - 1) / kTile;
   const int ntiles = dO ? a.ntx * ((H + kTile - 1) / kTile) : 0;
   const int grid = a.np * a.ng + ntiles;
   if (!dP && loss_total) k_loss_total<<<1, 256, 0, s>>>(loss_pat, B, loss_total);
-  k_assemble<<<grid, 256, 0, s>>>(a);
+  if (fftshift_sign)
+    k_assemble<true, 2><<<grid, 256, 0, s>>>(a);  // fused path: M = N even
+  else if (pair == 2)
+    k_assemble<false, 2><<<grid, 256, 0, s>>>(a);
+  else
+    k_assemble<false, 1><<<grid, 256, 0, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 

@@ -8,15 +8,17 @@ constexpr int kTile = 32;   // canvas tile edge for dO
 constexpr int kGroup = 16;  // patterns per dP partial sum
 constexpr int kPixBlock = 256;  // probe pixels per dP block
 
-// number of arrival counters the dP reduction needs (zeroed by the fused kernel)
-inline int dp_counters(int M) { return (M * M + kPixBlock - 1) / kPixBlock; }
+// number of arrival counters the dP reduction needs for M x N windows (zeroed
+// before the first call; every call leaves them zeroed)
+inline int dp_counters(int M, int N) { return (M * N + kPixBlock - 1) / kPixBlock; }
 
 // dP (group partials, then the last-arriving block sums them in group order),
 // dO (tile owner sums in ascending pattern order) and the FP64 loss total in
-// one launch; any output may be null.  E' is only read.  `done` holds
-// dp_counters(M) zeroed counters and is left zeroed.
+// one launch; any output may be null.  E' is only read; with fftshift_sign
+// it carries the fused kernels' (-1)^(x+y) factor (M = N even).  `done` holds
+// dp_counters(M, N) zeroed counters and is left zeroed.
 int launch_assemble(const float2* Eb, const float2* O, const float2* P, const int2* tlb, int B, int H, int W,
-                    int M, float2* dO, float2* dP, float2* part, unsigned* done, const double* loss_pat,
-                    double* loss_total, bool accumulate, cudaStream_t s);
+                    int M, int N, bool fftshift_sign, float2* dO, float2* dP, float2* part, unsigned* done,
+                    const double* loss_pat, double* loss_total, bool accumulate, cudaStream_t s);
 
 }  // namespace pty

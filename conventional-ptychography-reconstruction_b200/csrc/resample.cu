@@ -29,6 +29,7 @@
 
 #include "common.cuh"
 #include "dft_regs.cuh"
+#include "line_fft.cuh"
 
 namespace pty {
 namespace rs {
@@ -273,41 +274,13 @@ bool supported(int n, int N) {
 // ---------------------------------------------------------------------------
 namespace rsg {
 
-constexpr int kMaxFactors = 16;
-constexpr int kMaxLen = 8192;
-constexpr int kNT = 512;
+using lfft::LinePlan;
+using lfft::make_plan;
+using lfft::kMaxLen;
+using lfft::pad16;
+using lfft::transform;
+constexpr int kNT = lfft::kLineNT;
 constexpr size_t kSmemCap = 200 * 1024;
-
-struct LinePlan {
-  int L;
-  int nf;
-  int radix[kMaxFactors];
-};
-
-// factor L into passes: powers of two as 16, 8, 4, 2; then 3, 5, 7; any
-// other prime factor gets its own direct-sum pass
-static bool make_plan(int L, LinePlan* p) {
-  if (L < 1 || L > kMaxLen) return false;
-  p->L = L;
-  p->nf = 0;
-  int r = L;
-  auto push = [&](int f) {
-    if (p->nf >= kMaxFactors) return false;
-    p->radix[p->nf++] = f;
-    r /= f;
-    return true;
-  };
-  for (int f : {16, 8, 4, 2})
-    while (r % f == 0)
-      if (!push(f)) return false;
-  for (int f : {3, 5, 7})
-    while (r % f == 0)
-      if (!push(f)) return false;
-  for (int f = 11; r > 1; f += 2)
-    while (r % f == 0)
-      if (!push(f)) return false;
-  return true;
-}
 
 struct Args {
   const float2* in;
@@ -321,98 +294,6 @@ struct Args {
   int d, lo;        // band remap offset and lowest band frequency
   float scale;
 };
-
-__host__ __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
-
-template <int R, bool INV>
-PTY_DEVI void pass_r(const float2* __restrict__ src, float2* __restrict__ dst, const float2* __restrict__ tw,
-                     int L, int NS, int lines, int ls, int lmax, int t) {
-  const int bpl = L / R;
-  const int tws = lmax / (NS * R);
-  for (int b = t; b < lines * bpl; b += kNT) {
-    const int line = b / bpl, j = b - line * bpl;
-    const int k = j % NS;
-    const float2* sl = src + line * ls;
-    float2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = sl[pad16(j + r * bpl)];
-    if (NS > 1) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = tw[k * r * tws];
-        if (INV) w.y = -w.y;
-        v[r] = c_mul(v[r], w);
-      }
-    }
-    dft<R, INV, 1>(v);
-    float2* dl = dst + line * ls;
-    const int o = (j / NS) * NS * R + k;
-#pragma unroll
-    for (int r = 0; r < R; ++r) dl[pad16(o + r * NS)] = v[r];
-  }
-}
-
-// direct sum for a prime factor p: output o = (j / NS) NS p + k + r NS gets
-// sum_m x[j + m L/p] exp(-+2 pi i m (k + r NS) / (NS p))
-template <bool INV>
-PTY_DEVI void pass_generic(const float2* __restrict__ src, float2* __restrict__ dst, const float2* __restrict__ tw,
-                           int L, int p, int NS, int lines, int ls, int lmax, int t) {
-  const int bpl = L / p;
-  const int blk = NS * p;
-  const int tws = lmax / blk;
-  for (int e = t; e < lines * L; e += kNT) {
-    const int line = e / L, o = e - line * L;
-    const int ob = o / blk, rem = o - ob * blk;
-    const int r = rem / NS, k = rem - r * NS;
-    const int j = ob * NS + k;
-    const int q = (k + r * NS) * tws;  // < lmax
-    const float2* sl = src + line * ls;
-    float2 acc = make_float2(0.f, 0.f);
-    int idx = 0;
-    for (int m = 0; m < p; ++m) {
-      float2 w = tw[idx];
-      if (INV) w.y = -w.y;
-      const float2 x = sl[pad16(j + m * bpl)];
-      acc.x = fmaf(x.x, w.x, fmaf(-x.y, w.y, acc.x));
-      acc.y = fmaf(x.x, w.y, fmaf(x.y, w.x, acc.y));
-      idx += q;
-      if (idx >= lmax) idx -= lmax;
-    }
-    dst[line * ls + pad16(o)] = acc;
-  }
-}
-
-template <bool INV>
-PTY_DEVI void run_pass(int R, const float2* src, float2* dst, const float2* tw, int L, int NS, int lines, int ls,
-                       int lmax, int t) {
-  switch (R) {
-    case 2: pass_r<2, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    case 3: pass_r<3, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    case 4: pass_r<4, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    case 5: pass_r<5, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    case 7: pass_r<7, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    case 8: pass_r<8, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    case 16: pass_r<16, INV>(src, dst, tw, L, NS, lines, ls, lmax, t); break;
-    default: pass_generic<INV>(src, dst, tw, L, R, NS, lines, ls, lmax, t); break;
-  }
-}
-
-// all passes of one plan; returns the buffer that holds the result
-template <bool INV>
-PTY_DEVI float2* transform(const LinePlan& pl, float2* a, float2* b, const float2* tw, int lines, int ls, int lmax,
-                           int t) {
-  int NS = 1;
-  for (int i = 0; i < pl.nf; ++i) {
-    const int R = pl.radix[i];
-    run_pass<INV>(R, a, b, tw, pl.L, NS, lines, ls, lmax, t);
-    __syncthreads();
-    NS *= R;
-    float2* c = a;
-    a = b;
-    b = c;
-  }
-  return a;
-}
 
 template <bool COL>
 __global__ void __launch_bounds__(kNT) k_resample_any(const Args g) {

@@ -28,7 +28,8 @@ from . import _lib
 
 LOSS_CODES = {"smooth_L1_loss": 0, "FD_loss": 1, "Poisson_likelihood_loss": 2}
 _INTENSITY_GRAD = 3
-SUPPORTED_PROBE_SIZES = (64, 128, 256)
+FUSED_PROBE_SIZES = (64, 128, 256)  # square probes that run the fused kernels
+MAX_PROBE_DIM = 4096                 # any other 1 <= M, N <= 4096 runs the general path
 
 
 # --------------------------------------------------------------------------
@@ -64,13 +65,14 @@ def make_windows(tlY, tlX, device=None) -> torch.Tensor:
     return t.to(device) if device is not None else t
 
 
-def check_windows(tl: torch.Tensor, canvas_hw, M: int) -> None:
-    """Host-side bounds check of scan windows (raises ``ValueError``)."""
+def check_windows(tl: torch.Tensor, canvas_hw, M: int, N: int | None = None) -> None:
+    """Host-side bounds check of scan windows of M x N (N defaults to M; raises ``ValueError``)."""
     H, W = canvas_hw
+    N = M if N is None else N
     t = tl.detach().to("cpu")
     if t.numel() == 0:
         return
-    bad = (t[:, 0] < 0) | (t[:, 1] < 0) | (t[:, 0] > H - M) | (t[:, 1] > W - M)
+    bad = (t[:, 0] < 0) | (t[:, 1] < 0) | (t[:, 0] > H - M) | (t[:, 1] > W - N)
     if bool(bad.any()):
         i = int(torch.nonzero(bad)[0, 0])
         raise ValueError(f"scan window {i} at {t[i].tolist()} leaves the {H}x{W} canvas (probe {M})")
@@ -105,11 +107,12 @@ def _as_c64(x: torch.Tensor, name: str) -> torch.Tensor:
     return x.contiguous()
 
 
-def _check_probe(P: torch.Tensor) -> int:
-    if P.dim() != 2 or P.shape[0] != P.shape[1] or P.shape[0] not in SUPPORTED_PROBE_SIZES:
-        raise ValueError(f"probe must be square with size in {SUPPORTED_PROBE_SIZES}, got "
-                         f"{tuple(P.shape)}")
-    return int(P.shape[0])
+def _check_probe(P: torch.Tensor):
+    """(M, N) of a probe: square 64 / 128 / 256 run the fused kernels, any
+    other 1 <= M, N <= MAX_PROBE_DIM the general path."""
+    if P.dim() != 2 or not (1 <= P.shape[0] <= MAX_PROBE_DIM and 1 <= P.shape[1] <= MAX_PROBE_DIM):
+        raise ValueError(f"probe must be [M, N] with 1 <= M, N <= {MAX_PROBE_DIM}, got {tuple(P.shape)}")
+    return int(P.shape[0]), int(P.shape[1])
 
 
 _status_cache: dict = {}
@@ -153,7 +156,7 @@ class FwdAdjWorkspace:
 
 
 _default_ws: dict = {}
-_ws_size_cache: dict = {}  # (H, W, M, B) -> ptycho_fwd_adj_workspace_size
+_ws_size_cache: dict = {}  # (H, W, M, N, B) -> ptycho_fwd_adj_workspace_size
 
 
 def _batch_arg(batch, dev):
@@ -163,24 +166,32 @@ def _batch_arg(batch, dev):
 
 
 def forward_intensity(O: torch.Tensor, P: torch.Tensor, tl: torch.Tensor, batch=None) -> torch.Tensor:
-    """Far-field intensities ``[B, M, M]`` float32 (no autograd).
+    """Far-field intensities ``[B, M, N]`` float32 (no autograd).
 
     ``tl`` [F, 2] int32 windows of all frames; ``batch`` [B] frame ids (None:
     all F frames in order)."""
     O = _as_c64(O, "object")
     P = _as_c64(P, "probe")
-    M = _check_probe(P)
+    M, N = _check_probe(P)
     H, W = O.shape
     tl = tl.to(device=O.device, dtype=torch.int32).contiguous()
     F = int(tl.shape[0])
     bt = _batch_arg(batch, O.device)
     B = F if bt is None else int(bt.numel())
-    out = torch.empty((B, M, M), dtype=torch.float32, device=O.device)
+    out = torch.empty((B, M, N), dtype=torch.float32, device=O.device)
     st = device_status(O.device)
-    _lib.check(_lib.lib().ptycho_forward_intensity(
-        O.data_ptr(), H, W, P.data_ptr(), M, M, tl.data_ptr(), F,
-        bt.data_ptr() if bt is not None else None, B, out.data_ptr(), st.data_ptr(),
-        _stream_handle(O.device)), "ptycho_forward_intensity")
+    L = _lib.lib()
+    bp = bt.data_ptr() if bt is not None else None
+    if M == N and M in FUSED_PROBE_SIZES:
+        _lib.check(L.ptycho_forward_intensity(O.data_ptr(), H, W, P.data_ptr(), M, N, tl.data_ptr(), F, bp, B,
+                                              out.data_ptr(), st.data_ptr(), _stream_handle(O.device)),
+                   "ptycho_forward_intensity")
+    else:
+        ws = torch.empty(max(int(L.ptycho_forward_intensity_workspace_size(M, N, B)), 256), dtype=torch.uint8,
+                         device=O.device)
+        _lib.check(L.ptycho_forward_intensity_ws(O.data_ptr(), H, W, P.data_ptr(), M, N, tl.data_ptr(), F, bp, B,
+                                                 out.data_ptr(), ws.data_ptr(), ws.numel(), st.data_ptr(),
+                                                 _stream_handle(O.device)), "ptycho_forward_intensity_ws")
     return out
 
 
@@ -189,21 +200,21 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
                 workspace: "FwdAdjWorkspace | None" = None):
     """One call of ``ptycho_fwd_adj``.  Returns ``(loss_total, loss_per_pattern|None, dO, dP)``.
 
-    ``tl`` [F, 2] int32 and ``Imeas`` [F, M, M] float32 describe all frames;
+    ``tl`` [F, 2] int32 and ``Imeas`` [F, M, N] float32 describe all frames;
     ``batch`` [B] selects the frames of this call (None: all, in order).
     ``loss_total`` is a 0-d float64 CUDA tensor.  Gradient buffers are
     allocated unless given (``accumulate`` adds into given buffers)."""
     O = _as_c64(O, "object")
     P = _as_c64(P, "probe")
-    M = _check_probe(P)
+    M, N = _check_probe(P)
     H, W = O.shape
     dev = O.device
     tl = _i32(tl, dev)
     F = int(tl.shape[0])
     if Imeas.dtype != torch.float32 or not Imeas.is_contiguous() or Imeas.device != dev:
         Imeas = Imeas.to(device=dev, dtype=torch.float32).contiguous()
-    if Imeas.shape != (F, M, M):
-        raise ValueError(f"measurements must be [F, M, M] = {(F, M, M)}, got {tuple(Imeas.shape)}")
+    if Imeas.shape != (F, M, N):
+        raise ValueError(f"measurements must be [F, M, N] = {(F, M, N)}, got {tuple(Imeas.shape)}")
     bt = _batch_arg(batch, dev)
     B = F if bt is None else int(bt.numel())
     stream = _stream_handle(dev)
@@ -213,13 +224,13 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
         if dO is None:
             dO = torch.empty((H, W), dtype=torch.complex64, device=dev)
         if dP is None:
-            dP = torch.empty((M, M), dtype=torch.complex64, device=dev)
+            dP = torch.empty((M, N), dtype=torch.complex64, device=dev)
     else:
         dO = dP = None
-    key = (H, W, M, B)
+    key = (H, W, M, N, B)
     ws_bytes = _ws_size_cache.get(key)
     if ws_bytes is None:
-        ws_bytes = _ws_size_cache[key] = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, M, B))
+        ws_bytes = _ws_size_cache[key] = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, N, B))
     if workspace is None:
         # one default workspace per (device, stream): calls on one stream are
         # ordered, calls on different streams must not share scratch
@@ -229,7 +240,7 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
     ws = workspace.get(ws_bytes, dev)
     st = device_status(dev)
     _lib.check(_lib.lib().ptycho_fwd_adj(
-        O.data_ptr(), H, W, P.data_ptr(), M, M, tl.data_ptr(), Imeas.data_ptr(), F,
+        O.data_ptr(), H, W, P.data_ptr(), M, N, tl.data_ptr(), Imeas.data_ptr(), F,
         bt.data_ptr() if bt is not None else None, B, int(loss_code),
         lp.data_ptr() if lp is not None else None, loss_total.data_ptr(),
         dO.data_ptr() if dO is not None else None, dP.data_ptr() if dP is not None else None,
@@ -254,25 +265,25 @@ class FwdAdjPlan:
                             ("windows", tl, torch.int32), ("measurements", Imeas, torch.float32)):
             if not x.is_cuda or x.dtype != dt or not x.is_contiguous():
                 raise ValueError(f"{name} must be a contiguous CUDA {dt} tensor")
-        self.M = _check_probe(P)
+        self.M, self.N = _check_probe(P)
         self.O, self.P, self.tl, self.Imeas = O, P, tl, Imeas
         self.dev = O.device
         H, W = O.shape
         F = int(tl.shape[0])
-        if Imeas.shape != (F, self.M, self.M):
-            raise ValueError("measurements must be [F, M, M]")
+        if Imeas.shape != (F, self.M, self.N):
+            raise ValueError("measurements must be [F, M, N]")
         self.B = int(batch_size)
         self.batch = torch.zeros(self.B, dtype=torch.int32, device=self.dev)
         self.loss_total = torch.zeros((), dtype=torch.float64, device=self.dev)
         self.loss_per_pattern = (torch.zeros(self.B, dtype=torch.float64, device=self.dev)
                                  if per_pattern else None)
         self.dO = torch.zeros((H, W), dtype=torch.complex64, device=self.dev) if want_dO else None
-        self.dP = torch.zeros((self.M, self.M), dtype=torch.complex64, device=self.dev) if want_dP else None
-        nbytes = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, self.M, self.M, self.B))
+        self.dP = torch.zeros((self.M, self.N), dtype=torch.complex64, device=self.dev) if want_dP else None
+        nbytes = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, self.M, self.N, self.B))
         self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.dev)
         self.status = device_status(self.dev)
         ptr = lambda x: x.data_ptr() if x is not None else None  # noqa: E731
-        self._args = (O.data_ptr(), H, W, P.data_ptr(), self.M, self.M, tl.data_ptr(), Imeas.data_ptr(), F,
+        self._args = (O.data_ptr(), H, W, P.data_ptr(), self.M, self.N, tl.data_ptr(), Imeas.data_ptr(), F,
                       self.batch.data_ptr(), self.B, LOSS_CODES[loss_type], ptr(self.loss_per_pattern),
                       self.loss_total.data_ptr(), ptr(self.dO), ptr(self.dP), 0, self.ws.data_ptr(),
                       self.ws.numel(), self.status.data_ptr())
@@ -340,7 +351,7 @@ def fused_loss(object_complex: torch.Tensor, probe_complex: torch.Tensor, tl: to
                Imeas: torch.Tensor, loss_type: str = "smooth_L1_loss", batch=None) -> torch.Tensor:
     """Sum over the batch of the per-pattern mean loss (Recovery.py:288-307).
 
-    ``tl`` [F, 2] int32 (tlY, tlX) and ``Imeas`` [F, M, M] float32 for all
+    ``tl`` [F, 2] int32 (tlY, tlX) and ``Imeas`` [F, M, N] float32 for all
     frames; ``batch`` [B] frame ids of this minibatch (None: all frames).
     Returns a 0-d float64 tensor; ``backward()`` deposits dO / dP (torch's
     complex convention) into the inputs that require grad."""
@@ -366,7 +377,7 @@ class _ForwardIntensity(torch.autograd.Function):
 
 
 def forward_intensity_batched(O: torch.Tensor, P: torch.Tensor, tl: torch.Tensor) -> torch.Tensor:
-    """Differentiable batched intensities [B, M, M] (backward through the adjoint kernel)."""
+    """Differentiable batched intensities [B, M, N] (backward through the adjoint kernel)."""
     return _ForwardIntensity.apply(O, P, tl)
 
 
@@ -379,5 +390,5 @@ def forward_imaging_model(object_complex, probe_complex, tlY, tlX, brY, brX):
     if (M, N) != tuple(probe_complex.shape):
         raise ValueError(f"window {(M, N)} does not match probe {tuple(probe_complex.shape)}")
     tl = torch.tensor([[int(tlY), int(tlX)]], dtype=torch.int32, device=object_complex.device)
-    check_windows(tl, object_complex.shape, M)
+    check_windows(tl, object_complex.shape, M, N)
     return forward_intensity_batched(object_complex, probe_complex, tl)[0]

@@ -156,7 +156,7 @@ class Trainer:
             self.steps = scan_shards.steps_per_epoch(int(stack.shape[0]), self.world, int(batch_size))
             self.np_rng = np.random.default_rng(seed + self.rank)
         self.model = model
-        self.stack = stack  # [F, M, M] float32, device
+        self.stack = stack  # [F, M, N] float32, device
         self.tl = tl        # [F, 2] int32, device
         self.F = int(stack.shape[0])
         self.loss_type = loss_type
@@ -326,7 +326,7 @@ def main(argv=None):
         data["xlocation"], data["ylocation"], probe.shape, cfg["wavelength"], cfg["camera_length"],
         cfg["camera_pixel_pitch"])
     tl = optics.make_windows(tlY, tlX, dev)
-    optics.check_windows(tl, (canvas, canvas), probe.shape[0])
+    optics.check_windows(tl, (canvas, canvas), probe.shape[0], probe.shape[1])
     init_probe = data.get("initProbe", probe) if cfg.get("init_type", "initNone") == "initProbe" else None
     if cfg.get("init_type") == "initQuadratic":
         M, N = probe.shape

@@ -35,7 +35,7 @@ typedef struct CUstream_st* ptycho_stream_t; /* same type as cudaStream_t */
 typedef enum {
   PTYCHO_OK = 0,
   PTYCHO_ERR_INVALID_ARG = 1,      /* null pointer, negative size, bad enum */
-  PTYCHO_ERR_UNSUPPORTED_SIZE = 2, /* probe size not in {64,128,256}, M != N */
+  PTYCHO_ERR_UNSUPPORTED_SIZE = 2, /* size outside what the entry point takes */
   PTYCHO_ERR_MISALIGNED = 3,       /* pointer not aligned as documented */
   PTYCHO_ERR_WORKSPACE = 4,        /* workspace too small */
   PTYCHO_ERR_LAUNCH = 5,           /* CUDA launch failed (see cudaGetLastError) */
@@ -80,12 +80,25 @@ int ptycho_version(void);
  * batched: for b < B, with f = batch[b],
  *   I_out[b] = | fftshift( fft2( P * O[tlY_f : tlY_f+M, tlX_f : tlX_f+N] ) ) |^2
  * O [H][W] complex64, P [M][N] complex64, I_out [B][M][N] float32.
- * Supported: M == N in {64, 128, 256} (256: one 4-CTA thread-block cluster
- * per pattern).  Needs no scratch memory.
+ * ptycho_forward_intensity takes M == N in {64, 128, 256} (the fused
+ * kernels; 256: one 4-CTA thread-block cluster per pattern) and needs no
+ * scratch memory; other shapes return PTYCHO_ERR_UNSUPPORTED_SIZE.
+ * ptycho_forward_intensity_ws takes any 1 <= M, N <= 4096 (the reference
+ * accepts any probe shape, Recovery.py:290): shapes the fused kernels do not
+ * cover run as gather, mixed-radix row and column DFTs and an intensity
+ * pass over a workspace of ptycho_forward_intensity_workspace_size(M, N, B)
+ * bytes (256-byte aligned; the fused shapes need none).
  * ---------------------------------------------------------------------- */
 int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M, int N,
                              const int32_t* tl, int F, const int32_t* batch, int B,
                              float* I_out, int32_t* status_out, ptycho_stream_t stream);
+
+size_t ptycho_forward_intensity_workspace_size(int M, int N, int B);
+
+int ptycho_forward_intensity_ws(const float* O, int H, int W, const float* P, int M, int N,
+                                const int32_t* tl, int F, const int32_t* batch, int B, float* I_out,
+                                void* workspace, size_t workspace_bytes, int32_t* status_out,
+                                ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
  * Fused forward + loss + adjoint.  Replaces the per-frame loop of
@@ -102,7 +115,10 @@ int ptycho_forward_intensity(const float* O, int H, int W, const float* P, int M
  * added to instead of overwritten.  workspace: device scratch of at least
  * ptycho_fwd_adj_workspace_size() bytes, 256-byte aligned.  Imeas must be
  * 16-byte aligned (each pattern's measurement is fetched by a bulk copy).
- * M == N in {64, 128, 256}.
+ * Probes: M == N in {64, 128, 256} run the fused kernels; any other
+ * 1 <= M, N <= 4096 (non-square, odd, 96, 192, ...) runs the general path:
+ * the same losses and gradients through workspace passes (gather, row and
+ * column DFTs of any length, loss, inverse DFTs), then the same assembly.
  * ---------------------------------------------------------------------- */
 size_t ptycho_fwd_adj_workspace_size(int H, int W, int M, int N, int B);
 

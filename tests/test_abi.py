@@ -42,12 +42,22 @@ def test_status_strings_and_version():
 def test_validation_before_device_work():
     L = load_pkg().lib()
     fake = ctypes.c_void_p(4096)  # never dereferenced: validation fails first
-    # unsupported probe size
-    assert L.ptycho_fwd_adj(fake, 256, 256, fake, 32, 32, fake, fake, 4, None, 4, 0, None, None, None,
+    # probe side past the general path's 4096 maximum
+    assert L.ptycho_fwd_adj(fake, 8192, 8192, fake, 5000, 5000, fake, fake, 4, None, 4, 0, None, None, None,
                             None, 0, fake, 1 << 30, None, None) == 2
-    # non-square probe
+    assert L.ptycho_fwd_adj_workspace_size(8192, 8192, 5000, 5000, 4) == 0
+    # shapes other than square 64 / 128 / 256 need the workspace entry point
     assert L.ptycho_forward_intensity(fake, 256, 256, fake, 64, 128, fake, 1, None, 1, fake, None,
                                       None) == 2
+    n = L.ptycho_forward_intensity_workspace_size(96, 80, 3)
+    assert n >= 3 * 96 * 80 * 8 and L.ptycho_forward_intensity_workspace_size(96, 80, -1) == 0
+    assert L.ptycho_forward_intensity_ws(fake, 256, 256, fake, 96, 80, fake, 3, None, 3, fake, fake, n - 8,
+                                         None, None) == 4
+    assert L.ptycho_forward_intensity_ws(fake, 256, 256, fake, 96, 80, fake, 3, None, 3, fake,
+                                         ctypes.c_void_p(4096 + 16), n, None, None) == 3
+    # the general path's workspace holds the FD planes on top of the exit waves
+    assert (L.ptycho_fwd_adj_workspace_size(256, 256, 96, 80, 8) >=
+            8 * 96 * 80 * (8 + 12) + L.ptycho_fwd_adj_workspace_size(256, 256, 64, 64, 0))
     # null object
     assert L.ptycho_forward_intensity(None, 256, 256, fake, 64, 64, fake, 1, None, 1, fake, None,
                                       None) == 1

@@ -96,3 +96,24 @@ def test_pixel_grid_residual_drops(rec, tmp_path):
     for _ in range(10):
         tr.epoch()
     assert tr.residual() < 0.5 * r0
+
+
+@pytest.mark.parametrize("model_type,iters", [("pixel_grid", 3), ("inr", 2)])
+def test_recovery_main_96_probe_without_torch_fft(rec, tmp_path, monkeypatch, model_type, iters):
+    """A 96 x 96 probe (the general forward / adjoint path) on the multiple-of-6
+    canvas scan_positions_to_pixels builds (odd INR object grid, mixed-radix
+    upsampling): the whole run reaches no torch.fft transform."""
+    from scipy.io import loadmat
+    d = _dataset(tmp_path, M=96, n=5, step=21)
+    assert d["canvas"] == 186  # a multiple of 6 whose half (the INR object grid, 93) is odd
+
+    def boom(*a, **k):
+        raise AssertionError("torch.fft reached on the product path")
+    for name in ("fft", "ifft", "fft2", "ifft2", "fftn", "ifftn"):
+        monkeypatch.setattr(torch.fft, name, boom)
+    out = tmp_path / f"out96_{model_type}"
+    rec.main(["--config", _config(tmp_path, d, model_type, iters, out)])
+    r = loadmat(out / "result.mat")
+    obj, probe = r["object_complex"], r["probe_complex"]
+    assert obj.shape == (d["canvas"], d["canvas"]) and probe.shape == (96, 96)
+    assert np.all(np.isfinite(obj)) and np.all(np.isfinite(probe))
