@@ -9,7 +9,7 @@ Workload (default ``c1``): 1536^2 complex64 object, 128^2 probe, 40 x 40 raster
 peak, batch 256 patterns per GPU, seeded synthetic data (the reference's
 datasets are not distributed).  One step = one minibatch: the fused
 forward/loss/adjoint kernel plus the deterministic dO/dP assembly (and, for
-N > 1, the NCCL all-reduce of dP and of the scanned canvas rows of dO --
+N > 1, the NCCL all-reduce of dP and the point-to-point halo exchange of dO --
 each rank draws its minibatch from its own band of the raster, so per-GPU
 work is fixed: weak scaling).  L2 is flushed (a 256 MiB
 write) before every timed step; step times are CUDA events on the launching
@@ -288,7 +288,7 @@ def run_ours(args):
     def step(i):
         plan.batch.copy_(batches[i])
         plan.replay()
-        exchange.all_reduce(dO, dP)  # N > 1: dO over the scanned rows, dP (NCCL)
+        exchange.all_reduce(dO, dP)  # N > 1: dO halo rows, dP all-reduce (NCCL)
         return plan.loss_total
 
     w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -454,6 +454,9 @@ def run_ours(args):
                 "data": "synthetic (seeded generator; reference datasets not distributed)",
                 "config": _config(w, B, args), "roofline": roof, "e2e": e2e,
                 "e2e_resident_stack": e2e_resident, "gpu_launches": launches,
+                "exchange": {"scheme": "dO halo rows point to point, dP all-reduce (NCCL)" if world > 1 else "none (one rank)",
+                             "bytes_per_step_per_rank": exchange.bytes_per_step(W, M, M),
+                             "full_band_all_reduce_bytes": 8 * (exchange.rows[1] - exchange.rows[0]) * W + 8 * M * M},
                 "clocks": clk.summary(note=f"sampled every 50 ms over the {args.steps} timed steps and "
                                            f"{n_settle} identical untimed steps on either side "
                                            f"(~{SETTLE_S:.1f} s each)")}

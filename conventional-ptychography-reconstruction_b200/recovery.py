@@ -141,8 +141,12 @@ class Trainer:
     rank (one process per GPU), each rank trains on its own band of the
     raster (``scan_shards``), every rank takes the same number of minibatches
     per epoch, and the parameter gradients are summed over the ranks after
-    each backward pass, so the model replicas stay identical.  That mode runs
-    eagerly (no CUDA graph holds a collective)."""
+    each backward pass.  A pixel-grid object's gradient is combined by the
+    halo exchange (only rows shared by neighbouring bands cross the link;
+    each rank's object is current on its band and ``current`` / ``residual``
+    gather it first), all other gradients by all-reduce, so the replicas that
+    the next forward reads stay identical.  That mode runs eagerly (no CUDA
+    graph holds a collective)."""
 
     def __init__(self, model, stack, tl, loss_type, batch_size, lr, lr_decay_step=10000, lr_decay_gamma=0.1,
                  sparsity_weight=0.0, seed=0, use_graph=True):
@@ -155,6 +159,10 @@ class Trainer:
             self.frames = scan_shards.shard_frames(tl_host[:, 0], tl_host[:, 1], self.world, self.rank)
             self.steps = scan_shards.steps_per_epoch(int(stack.shape[0]), self.world, int(batch_size))
             self.np_rng = np.random.default_rng(seed + self.rank)
+            # the halo exchange needs a row-local loss: the Haar term couples rows across band edges
+            self.halo = isinstance(model, PixelGrid) and float(sparsity_weight) == 0.0
+            self.exchange = scan_shards.GradientExchange(tl_host[:, 0], tl_host[:, 1], int(stack.shape[1]),
+                                                         halo=self.halo)
         self.model = model
         self.stack = stack  # [F, M, N] float32, device
         self.tl = tl        # [F, 2] int32, device
@@ -247,7 +255,10 @@ class Trainer:
             loss = loss + self.sparsity_weight * haar_sparsity(obj)
         loss.backward()
         if self.world > 1:
-            scan_shards.all_reduce_grads([p for p in self.model.parameters() if p.requires_grad])
+            if self.halo:
+                self.exchange.all_reduce(self.model.object.grad, self.model.probe.grad)
+            else:
+                scan_shards.all_reduce_grads([p for p in self.model.parameters() if p.requires_grad])
         self.opt.step()
         self.last_loss = loss.detach()
         return self.last_loss
@@ -265,8 +276,16 @@ class Trainer:
         if self.use_graph:
             self.opt.sync_lr()
 
+    def _gather(self):
+        """World > 1 with the halo exchange: assemble the whole object from the
+        ranks' owned rows (every rank calls this at the same point)."""
+        if self.world > 1 and self.halo:
+            with torch.no_grad():
+                self.exchange.gather_object(self.model.object.data)
+
     @torch.no_grad()
     def current(self):
+        self._gather()
         obj, probe = self.model()
         return obj.squeeze(), center_and_normalize_probe(probe.squeeze())
 
