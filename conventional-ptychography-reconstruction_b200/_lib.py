@@ -96,8 +96,43 @@ def lib() -> ctypes.CDLL:
                 fn = getattr(L, name)
                 fn.restype = res
                 fn.argtypes = args
+            _bind_fast(L)
             _lib = L
     return _lib
+
+
+# The per-minibatch entry points through the CPython fast-call module when it
+# is built (csrc/fastabi.c: no per-argument ctypes conversion), else through
+# ctypes.  Both call the same functions of the one loaded libptycho_b200.so.
+_fast = None
+
+
+def _bind_fast(L) -> None:
+    global _fast
+    try:
+        from . import _fastabi
+    except ImportError:
+        _fast = None
+        return
+    addr = lambda f: ctypes.cast(f, ctypes.c_void_p).value  # noqa: E731
+    _fastabi.bind(addr(L.ptycho_fwd_adj), addr(L.ptycho_scale_pair))
+    _fast = _fastabi
+
+
+def fwd_adj(*args) -> int:
+    """ptycho_fwd_adj with the argument list of include/ptycho_b200.h."""
+    lib()
+    if _fast is not None:
+        return _fast.fwd_adj(*args)
+    return _lib.ptycho_fwd_adj(*args)
+
+
+def scale_pair(*args) -> int:
+    """ptycho_scale_pair with the argument list of include/ptycho_b200.h."""
+    lib()
+    if _fast is not None:
+        return _fast.scale_pair(*args)
+    return _lib.ptycho_scale_pair(*args)
 
 
 class PtychoError(RuntimeError):

@@ -6,6 +6,8 @@ Every ``*.cu`` file in this folder is compiled by ``nvcc`` with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` into an object file
 under ``_build/`` and linked into ``../libptycho_b200.so``.  Objects are rebuilt
 when their source or any header in this folder (or ``include/``) is newer.
+``fastabi.c`` (a CPython fast-call binding of the per-step entry points) is
+compiled by the host C compiler into ``../_fastabi<EXT_SUFFIX>``.
 No GPU is needed: nvcc cross-compiles.
 """
 from __future__ import annotations
@@ -17,6 +19,7 @@ import os
 import shutil
 import subprocess
 import sys
+import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
@@ -57,6 +60,20 @@ def _compile(src: str, verbose: bool, force: bool) -> str:
     return obj
 
 
+def build_fastabi(force: bool = False) -> str:
+    """The CPython binding module (host C code, no CUDA)."""
+    src = os.path.join(HERE, "fastabi.c")
+    out = os.path.join(PKG, "_fastabi" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
+        return out
+    cc = os.environ.get("CC") or shutil.which("gcc") or "cc"
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-I" + sysconfig.get_paths()["include"], src, "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building {src} failed:\n{r.stdout}\n{r.stderr}")
+    return out
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(HERE, "*.cu")))
@@ -68,6 +85,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_fastabi(force)
     return OUT
 
 

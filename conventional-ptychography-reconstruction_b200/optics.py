@@ -150,9 +150,10 @@ class FwdAdjWorkspace:
 
     def get(self, nbytes: int, device) -> torch.Tensor:
         nbytes = max(int(nbytes), 256)
-        if self.buf is None or self.buf.numel() < nbytes or self.buf.device != torch.device(device):
-            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
-        return self.buf
+        buf = self.buf
+        if buf is None or buf.numel() < nbytes or buf.device != device:
+            buf = self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        return buf
 
 
 _default_ws: dict = {}
@@ -239,7 +240,7 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
             workspace = _default_ws.setdefault((dev, stream), FwdAdjWorkspace())
     ws = workspace.get(ws_bytes, dev)
     st = device_status(dev)
-    _lib.check(_lib.lib().ptycho_fwd_adj(
+    _lib.check(_lib.fwd_adj(
         O.data_ptr(), H, W, P.data_ptr(), M, N, tl.data_ptr(), Imeas.data_ptr(), F,
         bt.data_ptr() if bt is not None else None, B, int(loss_code),
         lp.data_ptr() if lp is not None else None, loss_total.data_ptr(),
@@ -294,7 +295,7 @@ class FwdAdjPlan:
         self.batch.copy_(torch.as_tensor(frame_ids).to(self.dev, torch.int32), non_blocking=True)
 
     def run(self) -> None:
-        _lib.check(_lib.lib().ptycho_fwd_adj(*self._args, _stream_handle(self.dev)), "ptycho_fwd_adj")
+        _lib.check(_lib.fwd_adj(*self._args, _stream_handle(self.dev)), "ptycho_fwd_adj")
 
     def capture(self) -> None:
         self.run()  # warm: sets kernel attributes outside capture
@@ -340,7 +341,7 @@ class _FusedLoss(torch.autograd.Function):
         # one launch scales both gradients by the upstream scalar (out of place:
         # the saved dO/dP stay valid for a second backward)
         ptr = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
-        _lib.check(_lib.lib().ptycho_scale_pair(
+        _lib.check(_lib.scale_pair(
             ptr(dO if gO is not None else None), ptr(gO), 2 * dO.numel() if gO is not None else 0,
             ptr(dP if gP is not None else None), ptr(gP), 2 * dP.numel() if gP is not None else 0,
             s.data_ptr(), _stream_handle(s.device)), "ptycho_scale_pair")

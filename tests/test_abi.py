@@ -158,3 +158,22 @@ def test_workspace_size_monotone():
     assert 0 < a < b
     assert a >= 256 * 128 * 128 * 8
     assert L.ptycho_fwd_adj_workspace_size(-1, 5, 64, 64, 1) == 0
+
+
+def test_fast_binding_matches_ctypes_validation():
+    """The CPython fast-call binding (csrc/fastabi.c) reaches the same library
+    functions as ctypes: validation failures return the same status codes."""
+    pkg = load_pkg()
+    L = pkg.lib()
+    lib = pkg._lib
+    assert lib._fast is not None, "the _fastabi module was not built"
+    fake = 4096
+    for args in [(fake, 8192, 8192, fake, 5000, 5000, fake, fake, 4, None, 4, 0, None, None, None, None, 0, fake,
+                  1 << 30, None, None),
+                 (fake, 256, 256, fake, 64, 64, fake, fake, 4, None, 4, 9, None, None, None, None, 0, fake,
+                  1 << 30, None, None),
+                 (fake, 256, 256, fake, 64, 64, fake, fake, 4, None, 4, 0, None, None, None, None, 0, fake, 16,
+                  None, None)]:
+        assert lib.fwd_adj(*args) == L.ptycho_fwd_adj(*args) != 0
+    assert lib.scale_pair(None, None, 0, None, None, 0, None, None) == L.ptycho_scale_pair(
+        None, None, 0, None, None, 0, None, None) == 1
