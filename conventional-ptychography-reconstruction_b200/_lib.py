@@ -59,6 +59,9 @@ SIGNATURES = {
                                           _c_int, _vp]),
     "ptycho_hashgrid_backward_planar": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float,
                                                  _vp, _c_int, _vp]),
+    "ptycho_hashgrid_grid_scratch_size": (_c_size, [_vp, _c_int, _c_int, _c_int]),
+    "ptycho_hashgrid_backward_grid": (_c_int, [_vp, _vp, _vp, _c_int, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
+                                               _c_float, _vp, _c_int, _vp, _c_size, _vp]),
     "ptycho_cmlp_packed_bytes": (_c_size, []),
     "ptycho_cmlp_grad_floats": (_c_int, []),
     "ptycho_cmlp_pack": (_c_int, [_vp] * 12 + [_vp]),

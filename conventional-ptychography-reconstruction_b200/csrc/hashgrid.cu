@@ -268,6 +268,363 @@ __global__ void __launch_bounds__(256) k_hash_bwd_thread(const int* __restrict__
   dtable[e] = r;
 }
 
+// ---------------------------------------------------------------------------
+// Grid backward.  When the coordinates are a tensor-product grid (coordinate
+// n = i * Bj + j at (ax0[j], ax1[i]), both axes non-decreasing -- an INR's
+// pixel centres), the contributors of one level's vertex (cx, cy) are the
+// rectangle of coordinates with ix0[j] in {cx - 1, cx} and iy1[i] in
+// {cy - 1, cy}: j in [lo0[cx - 1], lo0[cx + 1]), i in [lo1[cy - 1],
+// lo1[cy + 1]).  Phase 1 sums each vertex's rectangle with the forward's
+// bilinear weights (wx * wy, wx = 1 - fx on the cell's own corner, fx on the
+// next) into G[vertex]; phase 2 sums, per table entry, the G of the vertices
+// mapping to it (a hashed level's collisions, a dense level's far-edge
+// aliases) in the order of the vertex list sorted by entry.  Both phases have
+// fixed orders: deterministic, no atomics, and the only per-step state is
+// the per-axis tables and one list entry per vertex (the host builds them,
+// hashgrid.py GridPlan).
+// ---------------------------------------------------------------------------
+struct GridArgs {
+  const int* ix0;
+  const int* iy1;
+  const int* lo0;
+  const int* lo1;
+  const int* vstart;
+  const int* vorder;
+  const float* fx0;
+  const float* fy1;
+  const float* dfeat;
+  int planar;
+  int N, A, Bj, L;
+  int E0[kMaxLevels], E1[kMaxLevels];
+  int cw0[kMaxLevels], cw1[kMaxLevels];  // most axis values in one cell
+  int lo0off[kMaxLevels], lo1off[kMaxLevels];
+  long long voff[kMaxLevels + 1];
+  float2* G;
+};
+
+PTY_DEVI float2 grid_dfeat(const GridArgs& g, int l, int n) {
+  if (g.planar) {
+    const float* p = g.dfeat + size_t(2 * l) * g.N + n;
+    return make_float2(__ldg(p), __ldg(p + g.N));
+  }
+  return __ldg(reinterpret_cast<const float2*>(g.dfeat) + size_t(n) * g.L + l);
+}
+
+// level, cx, cy and the contributor ranges of global vertex v
+struct VertexRange {
+  int l, cx, cy, i0, i1, j0, j1;
+};
+PTY_DEVI VertexRange vertex_range(const GridArgs& g, long long v) {
+  VertexRange r;
+  int l = 0;
+  while (l + 1 < g.L && v >= g.voff[l + 1]) ++l;
+  const int local = int(v - g.voff[l]);
+  const int E0 = g.E0[l];
+  r.l = l;
+  r.cy = local / E0;
+  r.cx = local - r.cy * E0;
+  const int* lo0 = g.lo0 + g.lo0off[l];
+  const int* lo1 = g.lo1 + g.lo1off[l];
+  r.j0 = lo0[max(r.cx - 1, 0)];
+  r.j1 = lo0[r.cx + 1];
+  r.i0 = lo1[max(r.cy - 1, 0)];
+  r.i1 = lo1[r.cy + 1];
+  return r;
+}
+
+PTY_DEVI float axis_weight(const int* ix, const float* fx, int k, int c) {
+  const float f = __ldg(fx + k);
+  return __ldg(ix + k) == c ? 1.f - f : f;
+}
+
+// Sum over the flattened rectangle of vertex r: terms k = tid, tid + step, ...
+// (i = i0 + k / nj, j = j0 + k % nj), four terms' loads in flight, added in k
+// order per thread.  The row / column of the next term follow by a constant
+// increment (one division per thread).
+PTY_DEVI void rect_sum(const GridArgs& g, const VertexRange& r, int tid, int step, float& ax, float& ay) {
+  const int nj = r.j1 - r.j0, ni = r.i1 - r.i0;
+  const int total = ni * nj;
+  if (tid >= total) return;
+  const int* ix0 = g.ix0 + size_t(r.l) * g.Bj;
+  const float* fx0 = g.fx0 + size_t(r.l) * g.Bj;
+  const int* iy1 = g.iy1 + size_t(r.l) * g.A;
+  const float* fy1 = g.fy1 + size_t(r.l) * g.A;
+  const int dq = step / nj, dr = step - dq * nj;
+  int i = tid / nj, j = tid - (tid / nj) * nj;
+  int k = tid;
+  auto advance = [&]() {
+    k += step;
+    j += dr;
+    i += dq;
+    if (j >= nj) {
+      j -= nj;
+      ++i;
+    }
+  };
+  for (; k + 3 * step < total;) {
+    float w[4];
+    float2 d[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int ii = r.i0 + i, jj = r.j0 + j;
+      w[u] = axis_weight(ix0, fx0, jj, r.cx) * axis_weight(iy1, fy1, ii, r.cy);
+      d[u] = grid_dfeat(g, r.l, ii * g.Bj + jj);
+      advance();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      ax = fmaf(w[u], d[u].x, ax);
+      ay = fmaf(w[u], d[u].y, ay);
+    }
+  }
+  for (; k < total; advance()) {
+    const int ii = r.i0 + i, jj = r.j0 + j;
+    const float wt = axis_weight(ix0, fx0, jj, r.cx) * axis_weight(iy1, fy1, ii, r.cy);
+    const float2 d = grid_dfeat(g, r.l, ii * g.Bj + jj);
+    ax = fmaf(wt, d.x, ax);
+    ay = fmaf(wt, d.y, ay);
+  }
+}
+
+// G lanes per vertex (G = 1 .. 32, a power of two; 32 / G vertices per warp):
+// the group strides the flattened rectangle, then a fixed xor tree within it
+template <int G>
+__global__ void __launch_bounds__(256) k_gvert_group(const GridArgs g, long long v0, long long v1) {
+  const int t = threadIdx.x, gl = t % G;
+  const long long v = v0 + ((long long)blockIdx.x * 256 + t) / G;
+  const bool in = v < v1;
+  float ax = 0.f, ay = 0.f;
+  if (in) {
+    const VertexRange r = vertex_range(g, v);
+    rect_sum(g, r, gl, G, ax, ay);
+  }
+  if constexpr (G > 1) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+  }
+  if (in && gl == 0) g.G[v] = make_float2(ax, ay);
+}
+
+// Coarse levels (cw0 * cw1 >= 16) separably, since a term's weight is
+// wx(j, cx) * wy(i, cy):
+//   rows    H[i][cx] = sum over j in [lo0[cx - 1], lo0[cx + 1]) of wx g(i, j)
+//   columns G[cy][cx] = sum over i in [lo1[cy - 1], lo1[cy + 1]) of wy H[i][cx]
+// Each pass gives G lanes to one output (lanes stride the range, fixed xor
+// tree).  H [A][E0] lives in scratch after the vertex sums, one level at a time.
+template <int G>
+__global__ void __launch_bounds__(256) k_gsep_rows(const GridArgs g, int l, float2* __restrict__ H) {
+  const int t = threadIdx.x, gl = t % G;
+  const long long item = ((long long)blockIdx.x * 256 + t) / G;
+  const int E0 = g.E0[l];
+  const bool in = item < (long long)g.A * E0;
+  float ax = 0.f, ay = 0.f;
+  int i = 0, cx = 0;
+  if (in) {
+    i = int(item / E0);
+    cx = int(item - (long long)i * E0);
+    const int* lo0 = g.lo0 + g.lo0off[l];
+    const int j0 = lo0[max(cx - 1, 0)], j1 = lo0[cx + 1];
+    const int* ix0 = g.ix0 + size_t(l) * g.Bj;
+    const float* fx0 = g.fx0 + size_t(l) * g.Bj;
+    const int rowbase = i * g.Bj;
+    int j = j0 + gl;
+    for (; j + 3 * G < j1; j += 4 * G) {
+      float w[4];
+      float2 d[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        w[u] = axis_weight(ix0, fx0, j + u * G, cx);
+        d[u] = grid_dfeat(g, l, rowbase + j + u * G);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        ax = fmaf(w[u], d[u].x, ax);
+        ay = fmaf(w[u], d[u].y, ay);
+      }
+    }
+    for (; j < j1; j += G) {
+      const float w = axis_weight(ix0, fx0, j, cx);
+      const float2 d = grid_dfeat(g, l, rowbase + j);
+      ax = fmaf(w, d.x, ax);
+      ay = fmaf(w, d.y, ay);
+    }
+  }
+  if constexpr (G > 1) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+  }
+  if (in && gl == 0) H[item] = make_float2(ax, ay);
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_gsep_cols(const GridArgs g, int l, const float2* __restrict__ H) {
+  const int t = threadIdx.x, gl = t % G;
+  const long long item = ((long long)blockIdx.x * 256 + t) / G;
+  const int E0 = g.E0[l], E1 = g.E1[l];
+  const bool in = item < (long long)E0 * E1;
+  float ax = 0.f, ay = 0.f;
+  if (in) {
+    const int cy = int(item / E0), cx = int(item - (long long)cy * E0);
+    const int* lo1 = g.lo1 + g.lo1off[l];
+    const int i0 = lo1[max(cy - 1, 0)], i1 = lo1[cy + 1];
+    const int* iy1 = g.iy1 + size_t(l) * g.A;
+    const float* fy1 = g.fy1 + size_t(l) * g.A;
+    int i = i0 + gl;
+    for (; i + 3 * G < i1; i += 4 * G) {
+      float w[4];
+      float2 h[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        w[u] = axis_weight(iy1, fy1, i + u * G, cy);
+        h[u] = H[size_t(i + u * G) * E0 + cx];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        ax = fmaf(w[u], h[u].x, ax);
+        ay = fmaf(w[u], h[u].y, ay);
+      }
+    }
+    for (; i < i1; i += G) {
+      const float w = axis_weight(iy1, fy1, i, cy);
+      const float2 h = H[size_t(i) * E0 + cx];
+      ax = fmaf(w, h.x, ax);
+      ay = fmaf(w, h.y, ay);
+    }
+  }
+  if constexpr (G > 1) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+  }
+  if (in && gl == 0) g.G[g.voff[l] + item] = make_float2(ax, ay);
+}
+
+// lanes for a sum of about n terms: the power of two nearest n / 4 in 1 .. 32
+static int lanes_for_terms(double n) {
+  int G = 1;
+  while (G < 32 && 8.0 * G <= n) G *= 2;
+  return G;
+}
+
+// a level takes the separable passes when its cells hold at least 16 terms
+static bool separable_level(const int32_t* extents, int l) { return extents[4 * l + 2] * extents[4 * l + 3] >= 16; }
+
+// Fine levels (a few contributors per vertex): one CTA per kTX x kTY vertices of
+// level l.  The gradient sub-rectangle those vertices touch (rows i in
+// [lo1[cy0 - 1], lo1[cy0 + kTY + 1]), columns likewise) and its axis tables are
+// staged in shared memory with coalesced loads; each thread then sums its
+// vertex's rectangle from shared memory in row-major order.
+constexpr int kTX = 32, kTY = 8;
+constexpr size_t kTileSmemCap = 96 * 1024;
+
+__global__ void __launch_bounds__(256) k_gvert_tile(const GridArgs g, int l) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  const int E0 = g.E0[l], E1 = g.E1[l];
+  const int cx0 = blockIdx.x * kTX, cy0 = blockIdx.y * kTY;
+  const int* lo0 = g.lo0 + g.lo0off[l];
+  const int* lo1 = g.lo1 + g.lo1off[l];
+  const int j_lo = lo0[max(cx0 - 1, 0)], j_hi = lo0[min(cx0 + kTX + 1, E0)];
+  const int i_lo = lo1[max(cy0 - 1, 0)], i_hi = lo1[min(cy0 + kTY + 1, E1)];
+  const int nc = j_hi - j_lo, nr = i_hi - i_lo;
+  float* sre = reinterpret_cast<float*>(tsm);
+  float* sim = sre + nr * nc;
+  int* six = reinterpret_cast<int*>(sim + nr * nc);
+  float* sfx = reinterpret_cast<float*>(six + nc);
+  int* siy = reinterpret_cast<int*>(sfx + nc);
+  float* sfy = reinterpret_cast<float*>(siy + nr);
+  const int t = threadIdx.x;
+  for (int k = t; k < nc; k += 256) {
+    six[k] = __ldg(g.ix0 + size_t(l) * g.Bj + j_lo + k);
+    sfx[k] = __ldg(g.fx0 + size_t(l) * g.Bj + j_lo + k);
+  }
+  for (int k = t; k < nr; k += 256) {
+    siy[k] = __ldg(g.iy1 + size_t(l) * g.A + i_lo + k);
+    sfy[k] = __ldg(g.fy1 + size_t(l) * g.A + i_lo + k);
+  }
+  for (int k = t; k < nr * nc; k += 256) {
+    const int r = k / nc, c = k - (k / nc) * nc;
+    const float2 d = grid_dfeat(g, l, (i_lo + r) * g.Bj + j_lo + c);
+    sre[k] = d.x;
+    sim[k] = d.y;
+  }
+  __syncthreads();
+  const int cx = cx0 + (t % kTX), cy = cy0 + (t / kTX);
+  if (cx >= E0 || cy >= E1) return;
+  const int j0 = lo0[max(cx - 1, 0)] - j_lo, j1 = lo0[cx + 1] - j_lo;
+  const int i0 = lo1[max(cy - 1, 0)] - i_lo, i1 = lo1[cy + 1] - i_lo;
+  float ax = 0.f, ay = 0.f;
+  for (int i = i0; i < i1; ++i) {
+    const float fy = sfy[i];
+    const float wy = siy[i] == cy ? 1.f - fy : fy;
+    for (int j = j0; j < j1; ++j) {
+      const float fx = sfx[j];
+      const float w = (six[j] == cx ? 1.f - fx : fx) * wy;
+      ax = fmaf(w, sre[i * nc + j], ax);
+      ay = fmaf(w, sim[i * nc + j], ay);
+    }
+  }
+  g.G[g.voff[l] + (long long)cy * E0 + cx] = make_float2(ax, ay);
+}
+
+// shared memory of a tile of level l (rows and columns bounded by the cell widths)
+static size_t tile_smem(const GridArgs& g, int l) {
+  const size_t nc = size_t(kTX + 2) * g.cw0[l], nr = size_t(kTY + 2) * g.cw1[l];
+  return (2 * nr * nc + 2 * nc + 2 * nr) * 4;
+}
+
+// WPB warps (1 or 8) per vertex: the WPB * 32 threads stride the flattened
+// rectangle; fixed xor tree per warp, then the warps' partials in warp order
+template <int WPB>
+__global__ void __launch_bounds__(256) k_gvert_warp(const GridArgs g, long long v0, long long v1) {
+  __shared__ float2 part[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int slot = w / WPB, ww = w % WPB;  // 8 / WPB vertices per block
+  const long long v = v0 + (long long)blockIdx.x * (8 / WPB) + slot;
+  const bool in = v < v1;
+  float ax = 0.f, ay = 0.f;
+  if (in) {
+    const VertexRange r = vertex_range(g, v);
+    rect_sum(g, r, ww * 32 + lane, WPB * 32, ax, ay);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+  }
+  if (WPB == 1) {
+    if (in && lane == 0) g.G[v] = make_float2(ax, ay);
+    return;
+  }
+  if (lane == 0) part[w] = make_float2(ax, ay);
+  __syncthreads();
+  if (in && ww == 0 && lane == 0) {
+    float2 t = part[w];
+    for (int k = 1; k < WPB; ++k) t = c_add(t, part[w + k]);
+    g.G[v] = t;
+  }
+}
+
+// per table entry: the G of its vertices, in vertex-list order
+__global__ void __launch_bounds__(256) k_gentry(const int* __restrict__ vstart, const int* __restrict__ vorder,
+                                                const float2* __restrict__ G, int E, float2* __restrict__ dtable,
+                                                int accumulate) {
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  if (e >= E) return;
+  const int s0 = __ldg(vstart + e), s1 = __ldg(vstart + e + 1);
+  float2 r = make_float2(0.f, 0.f);
+  for (int k = s0; k < s1; ++k) r = c_add(r, G[__ldg(vorder + k)]);
+  if (accumulate) r = c_add(dtable[e], r);
+  dtable[e] = r;
+}
+
 }  // namespace pty
 
 using namespace pty;
@@ -395,6 +752,137 @@ int ptycho_hashgrid_backward_planar(const int32_t* start, const int32_t* item_pl
   if ((long long)2 * n_levels * N > 0x7fffffffll) return PTYCHO_ERR_UNSUPPORTED_SIZE;
   return hash_backward(true, start, item_planar, weight, dfeatures_planar, N, n_levels, log2_hashmap_size,
                        base_resolution, per_level_scale, dtable, accumulate, stream);
+}
+
+size_t ptycho_hashgrid_grid_scratch_size(const int32_t* extents, int n_levels, int A, int Bj) {
+  if (!extents || n_levels < 1 || n_levels > kMaxLevels || A < 1 || Bj < 1) return 0;
+  size_t n = 0, hmax = 0;
+  for (int l = 0; l < n_levels; ++l) {
+    if (extents[4 * l] < 1 || extents[4 * l + 1] < 1 || extents[4 * l + 2] < 1 || extents[4 * l + 3] < 1) return 0;
+    n += size_t(extents[4 * l]) * size_t(extents[4 * l + 1]);
+    if (separable_level(extents, l)) {
+      const size_t h = size_t(A) * size_t(extents[4 * l]);
+      hmax = h > hmax ? h : hmax;
+    }
+  }
+  return (n + hmax) * sizeof(float2);  // vertex sums, then the separable passes' H
+}
+
+int ptycho_hashgrid_backward_grid(const int32_t* grid_int, const float* grid_frac, const int32_t* extents, int A,
+                                  int Bj, const float* dfeatures, int planar, int n_levels, int log2_hashmap_size,
+                                  int base_resolution, float per_level_scale, float* dtable, int accumulate,
+                                  void* scratch, size_t scratch_bytes, ptycho_stream_t stream) {
+  LevelTable L;
+  int st = make_levels(n_levels, log2_hashmap_size, base_resolution, per_level_scale, &L);
+  if (st) return st;
+  if (!grid_int || !grid_frac || !extents || !dfeatures || !dtable || A < 1 || Bj < 1) return PTYCHO_ERR_INVALID_ARG;
+  const long long N = (long long)A * Bj;
+  if (N * 4 >= (1ll << 31) || (planar && 2ll * n_levels * N >= (1ll << 31))) return PTYCHO_ERR_UNSUPPORTED_SIZE;
+  const size_t need = ptycho_hashgrid_grid_scratch_size(extents, n_levels, A, Bj);
+  if (need == 0) return PTYCHO_ERR_INVALID_ARG;
+  if (!scratch || scratch_bytes < need) return PTYCHO_ERR_WORKSPACE;
+  if (!pty_aligned(dfeatures, planar ? 4 : 8) || !pty_aligned(dtable, 8) || !pty_aligned(scratch, 8) ||
+      !pty_aligned(grid_int, 4) || !pty_aligned(grid_frac, 4))
+    return PTYCHO_ERR_MISALIGNED;
+  GridArgs g{};
+  g.dfeat = dfeatures;
+  g.planar = planar ? 1 : 0;
+  g.N = int(N);
+  g.A = A;
+  g.Bj = Bj;
+  g.L = n_levels;
+  // layout of grid_int: ix0 [L][Bj], iy1 [L][A], lo0 [sum (E0 + 1)], lo1 [sum (E1 + 1)],
+  // vstart [entries + 1], vorder [vertices]; grid_frac: fx0 [L][Bj], fy1 [L][A]
+  size_t off = 0;
+  g.ix0 = grid_int + off;
+  off += size_t(n_levels) * Bj;
+  g.iy1 = grid_int + off;
+  off += size_t(n_levels) * A;
+  g.lo0 = grid_int + off;
+  int o0 = 0, o1 = 0;
+  long long nv = 0;
+  for (int l = 0; l < n_levels; ++l) {
+    g.E0[l] = extents[4 * l];
+    g.E1[l] = extents[4 * l + 1];
+    g.cw0[l] = extents[4 * l + 2];
+    g.cw1[l] = extents[4 * l + 3];
+    g.lo0off[l] = o0;
+    g.lo1off[l] = o1;
+    o0 += g.E0[l] + 1;
+    o1 += g.E1[l] + 1;
+    g.voff[l] = nv;
+    nv += (long long)g.E0[l] * g.E1[l];
+  }
+  g.voff[n_levels] = nv;
+  off += size_t(o0);
+  g.lo1 = grid_int + off;
+  off += size_t(o1);
+  g.vstart = grid_int + off;
+  off += size_t(L.total) + 1;
+  g.vorder = grid_int + off;
+  g.fx0 = grid_frac;
+  g.fy1 = grid_frac + size_t(n_levels) * Bj;
+  g.G = static_cast<float2*>(scratch);
+  // lanes per vertex by the level's average contributors per vertex: 256 (a
+  // block) from 2048 terms, else the power of two nearest terms / 4 in 1 .. 32
+  // (about four terms per lane); levels run coarse to fine, so equal choices
+  // form runs of levels, one launch each
+  auto lanes_for = [&](int l) {
+    const double terms = (2.0 * Bj / g.E0[l]) * (2.0 * A / g.E1[l]);
+    if (terms >= 2048.0) return 256;
+    int G = 1;
+    while (G < 32 && 4.0 * G * 2 <= terms) G *= 2;
+    return G;
+  };
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  float2* H = g.G + g.voff[n_levels];
+#define PTY_LANES(G, KERN, ITEMS, ...)                                                   \
+  switch (G) {                                                                         \
+    case 32: KERN<32><<<unsigned(((ITEMS) * 32 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break; \
+    case 16: KERN<16><<<unsigned(((ITEMS) * 16 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break; \
+    case 8: KERN<8><<<unsigned(((ITEMS) * 8 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;    \
+    case 4: KERN<4><<<unsigned(((ITEMS) * 4 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;    \
+    case 2: KERN<2><<<unsigned(((ITEMS) * 2 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;    \
+    default: KERN<1><<<unsigned(((ITEMS) + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;      \
+  }
+  for (int l0 = 0; l0 < n_levels;) {
+    if (separable_level(extents, l0)) {  // rows, then columns through H
+      const long long rows_items = (long long)A * g.E0[l0], col_items = (long long)g.E0[l0] * g.E1[l0];
+      const int Gr = lanes_for_terms(2.0 * Bj / g.E0[l0]), Gc = lanes_for_terms(2.0 * A / g.E1[l0]);
+      PTY_LANES(Gr, k_gsep_rows, rows_items, g, l0, H)
+      PTY_LANES(Gc, k_gsep_cols, col_items, g, l0, H)
+      ++l0;
+      continue;
+    }
+    const int G = lanes_for(l0);
+    // fine levels whose tile fits in shared memory: one tile launch per level
+    if (G <= 8 && tile_smem(g, l0) <= kTileSmemCap) {
+      const size_t smem = tile_smem(g, l0);
+      if (smem > 48 * 1024 &&
+          cudaFuncSetAttribute(k_gvert_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTileSmemCap)) !=
+              cudaSuccess)
+        return PTYCHO_ERR_LAUNCH;
+      const dim3 grid(unsigned((g.E0[l0] + kTX - 1) / kTX), unsigned((g.E1[l0] + kTY - 1) / kTY));
+      k_gvert_tile<<<grid, 256, smem, s>>>(g, l0);
+      ++l0;
+      continue;
+    }
+    int l1 = l0 + 1;
+    while (l1 < n_levels && lanes_for(l1) == G && !(G <= 8 && tile_smem(g, l1) <= kTileSmemCap) &&
+           !separable_level(extents, l1))
+      ++l1;
+    const long long va = g.voff[l0], vb = g.voff[l1], nvv = vb - va;
+    if (G == 256) {
+      k_gvert_warp<8><<<unsigned(nvv), 256, 0, s>>>(g, va, vb);
+    } else {
+      PTY_LANES(G, k_gvert_group, nvv, g, va, vb)
+    }
+    l0 = l1;
+  }
+#undef PTY_LANES
+  k_gentry<<<unsigned((L.total + 255) / 256), 256, 0, s>>>(g.vstart, g.vorder, g.G, L.total,
+                                                           reinterpret_cast<float2*>(dtable), accumulate);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
 }  // extern "C"

@@ -387,6 +387,33 @@ int ptycho_gs_backward(int kind, const float* xy, const float* p1, const float* 
                        float* dweight, ptycho_stream_t stream);
 
 /* ---------------------------------------------------------------------- *
+ * Hash-grid backward for coordinates on a tensor-product grid (an INR's pixel
+ * centres, models/complex_inr.py:179-205): coordinate n = i * Bj + j is
+ * (ax0[j], ax1[i]) with both axes non-decreasing.  Same result as
+ * ptycho_hashgrid_backward (the table gradient, deterministic), without the
+ * per-contribution CSR: every level's vertex sums the rectangle of
+ * coordinates whose cells touch it, then every entry sums its vertices.
+ * extents: HOST [n_levels][4] int32 per level: vertex extents E0, E1 and the
+ *   most axis values in one cell along each axis (cw0, cw1).  Coarse levels
+ *   (cw0 * cw1 >= 16) are summed separably: rows first (H[i][cx] = sum over
+ *   the cell pair of wx g), then columns (G = sum over rows of wy H); finer
+ *   levels per vertex.
+ * grid_int (device int32): ix0 [L][Bj], iy1 [L][A] (cell corners of the axis
+ *   values), lo0 [sum (E0+1)], lo1 [sum (E1+1)] (first axis index whose corner
+ *   is >= c), vstart [entries+1], vorder [vertices] (vertices sorted by entry);
+ * grid_frac (device float32): fx0 [L][Bj], fy1 [L][A] (cell fractions of
+ *   x * scale + 0.5 formed with one rounding).
+ * scratch: ptycho_hashgrid_grid_scratch_size(extents, n_levels, A, Bj) bytes.
+ * dfeatures [N][2L] or, with planar, feature-major [2L][N].
+ * ---------------------------------------------------------------------- */
+size_t ptycho_hashgrid_grid_scratch_size(const int32_t* extents, int n_levels, int A, int Bj);
+
+int ptycho_hashgrid_backward_grid(const int32_t* grid_int, const float* grid_frac, const int32_t* extents, int A,
+                                  int Bj, const float* dfeatures, int planar, int n_levels, int log2_hashmap_size,
+                                  int base_resolution, float per_level_scale, float* dtable, int accumulate,
+                                  void* scratch, size_t scratch_bytes, ptycho_stream_t stream);
+
+/* ---------------------------------------------------------------------- *
  * ptycho_fwd_adj without a workspace, for callers that cannot allocate
  * device memory (an FFI host with no CUDA allocator of its own, a step that
  * must not trigger an allocation's device synchronisation).  No counterpart
