@@ -300,6 +300,16 @@ struct GridArgs {
   int lo0off[kMaxLevels], lo1off[kMaxLevels];
   long long voff[kMaxLevels + 1];
   float2* G;
+  // the separable levels (k = 0 .. nsep-1): level, lanes of the row and column
+  // passes, offset of the level's rows in H, first block of each pass
+  int nsep;
+  int sep_l[kMaxLevels], sep_gr[kMaxLevels], sep_gc[kMaxLevels];
+  long long sep_h[kMaxLevels], sep_rb[kMaxLevels + 1], sep_cb[kMaxLevels + 1];
+  // the tiled fine levels: level, tiles per row, first block
+  int ntile;
+  int tile_l[kMaxLevels], tile_gx[kMaxLevels];
+  long long tile_b[kMaxLevels + 1];
+  float4* H;  // (S0, S1) row sums of the separable levels
 };
 
 PTY_DEVI float2 grid_dfeat(const GridArgs& g, int l, int n) {
@@ -409,68 +419,96 @@ __global__ void __launch_bounds__(256) k_gvert_group(const GridArgs g, long long
 }
 
 // Coarse levels (cw0 * cw1 >= 16) separably, since a term's weight is
-// wx(j, cx) * wy(i, cy):
-//   rows    H[i][cx] = sum over j in [lo0[cx - 1], lo0[cx + 1]) of wx g(i, j)
-//   columns G[cy][cx] = sum over i in [lo1[cy - 1], lo1[cy + 1]) of wy H[i][cx]
-// Each pass gives G lanes to one output (lanes stride the range, fixed xor
-// tree).  H [A][E0] lives in scratch after the vertex sums, one level at a time.
-template <int G>
-__global__ void __launch_bounds__(256) k_gsep_rows(const GridArgs g, int l, float2* __restrict__ H) {
-  const int t = threadIdx.x, gl = t % G;
-  const long long item = ((long long)blockIdx.x * 256 + t) / G;
+// wx(j, cx) * wy(i, cy).  Row pass: per row i and cell c (the j with
+// ix0[j] = c), S0 = sum (1 - fx) g and S1 = sum fx g, so every gradient value
+// is read once.  Column pass: G[cy][cx] = sum over i in [lo1[cy - 1],
+// lo1[cy + 1]) of wy (S1[i][cx - 1] + S0[i][cx]).  One launch per pass covers
+// every separable level (blocks by level); G lanes (uniform in a block) share
+// one output, striding its range, then a fixed xor tree.
+
+PTY_DEVI void lane_reduce(float& ax, float& ay, int G) {
+  for (int o = G >> 1; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+  }
+}
+
+// the separable level of block b of a pass whose levels start at `first`
+PTY_DEVI int sep_slot(const GridArgs& g, const long long* first, long long b) {
+  int k = 0;
+  while (k + 1 < g.nsep && b >= first[k + 1]) ++k;
+  return k;
+}
+
+__global__ void __launch_bounds__(256) k_gsep_rows(const GridArgs g) {
+  const long long b = blockIdx.x;
+  const int k = sep_slot(g, g.sep_rb, b);
+  const int l = g.sep_l[k], G = g.sep_gr[k];
+  const int t = threadIdx.x, gl = t & (G - 1);
+  const long long item = ((b - g.sep_rb[k]) * 256 + t) / G;
   const int E0 = g.E0[l];
   const bool in = item < (long long)g.A * E0;
-  float ax = 0.f, ay = 0.f;
-  int i = 0, cx = 0;
+  float s0x = 0.f, s0y = 0.f, s1x = 0.f, s1y = 0.f;
   if (in) {
-    i = int(item / E0);
-    cx = int(item - (long long)i * E0);
+    const int i = int(item / E0);
+    const int c = int(item - (long long)i * E0);
     const int* lo0 = g.lo0 + g.lo0off[l];
-    const int j0 = lo0[max(cx - 1, 0)], j1 = lo0[cx + 1];
-    const int* ix0 = g.ix0 + size_t(l) * g.Bj;
+    const int j0 = lo0[c], j1 = lo0[c + 1];
     const float* fx0 = g.fx0 + size_t(l) * g.Bj;
     const int rowbase = i * g.Bj;
     int j = j0 + gl;
     for (; j + 3 * G < j1; j += 4 * G) {
-      float w[4];
+      float f[4];
       float2 d[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        w[u] = axis_weight(ix0, fx0, j + u * G, cx);
+        f[u] = __ldg(fx0 + j + u * G);
         d[u] = grid_dfeat(g, l, rowbase + j + u * G);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        ax = fmaf(w[u], d[u].x, ax);
-        ay = fmaf(w[u], d[u].y, ay);
+        const float w0 = 1.f - f[u];
+        s0x = fmaf(w0, d[u].x, s0x);
+        s0y = fmaf(w0, d[u].y, s0y);
+        s1x = fmaf(f[u], d[u].x, s1x);
+        s1y = fmaf(f[u], d[u].y, s1y);
       }
     }
     for (; j < j1; j += G) {
-      const float w = axis_weight(ix0, fx0, j, cx);
+      const float f = __ldg(fx0 + j);
       const float2 d = grid_dfeat(g, l, rowbase + j);
-      ax = fmaf(w, d.x, ax);
-      ay = fmaf(w, d.y, ay);
+      s0x = fmaf(1.f - f, d.x, s0x);
+      s0y = fmaf(1.f - f, d.y, s0y);
+      s1x = fmaf(f, d.x, s1x);
+      s1y = fmaf(f, d.y, s1y);
     }
   }
-  if constexpr (G > 1) {
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) {
-      ax += __shfl_xor_sync(0xffffffffu, ax, o);
-      ay += __shfl_xor_sync(0xffffffffu, ay, o);
-    }
-  }
-  if (in && gl == 0) H[item] = make_float2(ax, ay);
+  lane_reduce(s0x, s0y, G);
+  lane_reduce(s1x, s1y, G);
+  if (in && gl == 0) g.H[g.sep_h[k] + item] = make_float4(s0x, s0y, s1x, s1y);
 }
 
-template <int G>
-__global__ void __launch_bounds__(256) k_gsep_cols(const GridArgs g, int l, const float2* __restrict__ H) {
-  const int t = threadIdx.x, gl = t % G;
-  const long long item = ((long long)blockIdx.x * 256 + t) / G;
+__global__ void __launch_bounds__(256) k_gsep_cols(const GridArgs g) {
+  const long long b = blockIdx.x;
+  const int k = sep_slot(g, g.sep_cb, b);
+  const int l = g.sep_l[k], G = g.sep_gc[k];
+  const int t = threadIdx.x, gl = t & (G - 1);
+  const long long item = ((b - g.sep_cb[k]) * 256 + t) / G;
   const int E0 = g.E0[l], E1 = g.E1[l];
   const bool in = item < (long long)E0 * E1;
+  const float4* H = g.H + g.sep_h[k];
   float ax = 0.f, ay = 0.f;
   if (in) {
     const int cy = int(item / E0), cx = int(item - (long long)cy * E0);
+    auto Hat = [&](int i) {  // H[i][cx] = S1[i][cx - 1] + S0[i][cx]
+      const float4 a0 = H[size_t(i) * E0 + cx];
+      float2 h = make_float2(a0.x, a0.y);
+      if (cx > 0) {
+        const float4 a1 = H[size_t(i) * E0 + cx - 1];
+        h = make_float2(a1.z + h.x, a1.w + h.y);
+      }
+      return h;
+    };
     const int* lo1 = g.lo1 + g.lo1off[l];
     const int i0 = lo1[max(cy - 1, 0)], i1 = lo1[cy + 1];
     const int* iy1 = g.iy1 + size_t(l) * g.A;
@@ -482,7 +520,7 @@ __global__ void __launch_bounds__(256) k_gsep_cols(const GridArgs g, int l, cons
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         w[u] = axis_weight(iy1, fy1, i + u * G, cy);
-        h[u] = H[size_t(i + u * G) * E0 + cx];
+        h[u] = Hat(i + u * G);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -492,18 +530,12 @@ __global__ void __launch_bounds__(256) k_gsep_cols(const GridArgs g, int l, cons
     }
     for (; i < i1; i += G) {
       const float w = axis_weight(iy1, fy1, i, cy);
-      const float2 h = H[size_t(i) * E0 + cx];
+      const float2 h = Hat(i);
       ax = fmaf(w, h.x, ax);
       ay = fmaf(w, h.y, ay);
     }
   }
-  if constexpr (G > 1) {
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) {
-      ax += __shfl_xor_sync(0xffffffffu, ax, o);
-      ay += __shfl_xor_sync(0xffffffffu, ay, o);
-    }
-  }
+  lane_reduce(ax, ay, G);
   if (in && gl == 0) g.G[g.voff[l] + item] = make_float2(ax, ay);
 }
 
@@ -518,17 +550,22 @@ static int lanes_for_terms(double n) {
 static bool separable_level(const int32_t* extents, int l) { return extents[4 * l + 2] * extents[4 * l + 3] >= 16; }
 
 // Fine levels (a few contributors per vertex): one CTA per kTX x kTY vertices of
-// level l.  The gradient sub-rectangle those vertices touch (rows i in
+// a level, all tiled levels in one launch (blocks by level).  The gradient sub-rectangle those vertices touch (rows i in
 // [lo1[cy0 - 1], lo1[cy0 + kTY + 1]), columns likewise) and its axis tables are
 // staged in shared memory with coalesced loads; each thread then sums its
 // vertex's rectangle from shared memory in row-major order.
 constexpr int kTX = 32, kTY = 8;
 constexpr size_t kTileSmemCap = 96 * 1024;
 
-__global__ void __launch_bounds__(256) k_gvert_tile(const GridArgs g, int l) {
+__global__ void __launch_bounds__(256) k_gvert_tile(const GridArgs g) {
   extern __shared__ __align__(16) unsigned char tsm[];
+  const long long b = blockIdx.x;
+  int k = 0;
+  while (k + 1 < g.ntile && b >= g.tile_b[k + 1]) ++k;
+  const int l = g.tile_l[k];
+  const int bl = int(b - g.tile_b[k]);
   const int E0 = g.E0[l], E1 = g.E1[l];
-  const int cx0 = blockIdx.x * kTX, cy0 = blockIdx.y * kTY;
+  const int cx0 = (bl % g.tile_gx[k]) * kTX, cy0 = (bl / g.tile_gx[k]) * kTY;
   const int* lo0 = g.lo0 + g.lo0off[l];
   const int* lo1 = g.lo1 + g.lo1off[l];
   const int j_lo = lo0[max(cx0 - 1, 0)], j_hi = lo0[min(cx0 + kTX + 1, E0)];
@@ -541,19 +578,20 @@ __global__ void __launch_bounds__(256) k_gvert_tile(const GridArgs g, int l) {
   int* siy = reinterpret_cast<int*>(sfx + nc);
   float* sfy = reinterpret_cast<float*>(siy + nr);
   const int t = threadIdx.x;
-  for (int k = t; k < nc; k += 256) {
-    six[k] = __ldg(g.ix0 + size_t(l) * g.Bj + j_lo + k);
-    sfx[k] = __ldg(g.fx0 + size_t(l) * g.Bj + j_lo + k);
+  for (int q = t; q < nc; q += 256) {
+    six[q] = __ldg(g.ix0 + size_t(l) * g.Bj + j_lo + q);
+    sfx[q] = __ldg(g.fx0 + size_t(l) * g.Bj + j_lo + q);
   }
-  for (int k = t; k < nr; k += 256) {
-    siy[k] = __ldg(g.iy1 + size_t(l) * g.A + i_lo + k);
-    sfy[k] = __ldg(g.fy1 + size_t(l) * g.A + i_lo + k);
+  for (int q = t; q < nr; q += 256) {
+    siy[q] = __ldg(g.iy1 + size_t(l) * g.A + i_lo + q);
+    sfy[q] = __ldg(g.fy1 + size_t(l) * g.A + i_lo + q);
   }
-  for (int k = t; k < nr * nc; k += 256) {
-    const int r = k / nc, c = k - (k / nc) * nc;
-    const float2 d = grid_dfeat(g, l, (i_lo + r) * g.Bj + j_lo + c);
-    sre[k] = d.x;
-    sim[k] = d.y;
+  for (int r = t >> 5; r < nr; r += 8) {  // a warp per row, lanes along it
+    for (int c = t & 31; c < nc; c += 32) {
+      const float2 d = grid_dfeat(g, l, (i_lo + r) * g.Bj + j_lo + c);
+      sre[r * nc + c] = d.x;
+      sim[r * nc + c] = d.y;
+    }
   }
   __syncthreads();
   const int cx = cx0 + (t % kTX), cy = cy0 + (t / kTX);
@@ -756,16 +794,14 @@ int ptycho_hashgrid_backward_planar(const int32_t* start, const int32_t* item_pl
 
 size_t ptycho_hashgrid_grid_scratch_size(const int32_t* extents, int n_levels, int A, int Bj) {
   if (!extents || n_levels < 1 || n_levels > kMaxLevels || A < 1 || Bj < 1) return 0;
-  size_t n = 0, hmax = 0;
+  size_t n = 0, h = 0;
   for (int l = 0; l < n_levels; ++l) {
     if (extents[4 * l] < 1 || extents[4 * l + 1] < 1 || extents[4 * l + 2] < 1 || extents[4 * l + 3] < 1) return 0;
     n += size_t(extents[4 * l]) * size_t(extents[4 * l + 1]);
-    if (separable_level(extents, l)) {
-      const size_t h = size_t(A) * size_t(extents[4 * l]);
-      hmax = h > hmax ? h : hmax;
-    }
+    if (separable_level(extents, l)) h += size_t(A) * size_t(extents[4 * l]);
   }
-  return (n + hmax) * sizeof(float2);  // vertex sums, then the separable passes' H
+  // vertex sums (float2), then every separable level's (S0, S1) rows (float4)
+  return n * sizeof(float2) + 16 + h * sizeof(float4);
 }
 
 int ptycho_hashgrid_backward_grid(const int32_t* grid_int, const float* grid_frac, const int32_t* extents, int A,
@@ -835,51 +871,65 @@ int ptycho_hashgrid_backward_grid(const int32_t* grid_int, const float* grid_fra
     return G;
   };
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  float2* H = g.G + g.voff[n_levels];
-#define PTY_LANES(G, KERN, ITEMS, ...)                                                   \
-  switch (G) {                                                                         \
-    case 32: KERN<32><<<unsigned(((ITEMS) * 32 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break; \
-    case 16: KERN<16><<<unsigned(((ITEMS) * 16 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break; \
-    case 8: KERN<8><<<unsigned(((ITEMS) * 8 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;    \
-    case 4: KERN<4><<<unsigned(((ITEMS) * 4 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;    \
-    case 2: KERN<2><<<unsigned(((ITEMS) * 2 + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;    \
-    default: KERN<1><<<unsigned(((ITEMS) + 255) / 256), 256, 0, s>>>(__VA_ARGS__); break;      \
-  }
-  for (int l0 = 0; l0 < n_levels;) {
-    if (separable_level(extents, l0)) {  // rows, then columns through H
-      const long long rows_items = (long long)A * g.E0[l0], col_items = (long long)g.E0[l0] * g.E1[l0];
-      const int Gr = lanes_for_terms(2.0 * Bj / g.E0[l0]), Gc = lanes_for_terms(2.0 * A / g.E1[l0]);
-      PTY_LANES(Gr, k_gsep_rows, rows_items, g, l0, H)
-      PTY_LANES(Gc, k_gsep_cols, col_items, g, l0, H)
-      ++l0;
-      continue;
-    }
-    const int G = lanes_for(l0);
-    // fine levels whose tile fits in shared memory: one tile launch per level
-    if (G <= 8 && tile_smem(g, l0) <= kTileSmemCap) {
-      const size_t smem = tile_smem(g, l0);
-      if (smem > 48 * 1024 &&
-          cudaFuncSetAttribute(k_gvert_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTileSmemCap)) !=
-              cudaSuccess)
-        return PTYCHO_ERR_LAUNCH;
-      const dim3 grid(unsigned((g.E0[l0] + kTX - 1) / kTX), unsigned((g.E1[l0] + kTY - 1) / kTY));
-      k_gvert_tile<<<grid, 256, smem, s>>>(g, l0);
-      ++l0;
-      continue;
-    }
-    int l1 = l0 + 1;
-    while (l1 < n_levels && lanes_for(l1) == G && !(G <= 8 && tile_smem(g, l1) <= kTileSmemCap) &&
-           !separable_level(extents, l1))
-      ++l1;
-    const long long va = g.voff[l0], vb = g.voff[l1], nvv = vb - va;
-    if (G == 256) {
-      k_gvert_warp<8><<<unsigned(nvv), 256, 0, s>>>(g, va, vb);
+  g.H = reinterpret_cast<float4*>(pty_align_up(reinterpret_cast<uintptr_t>(g.G + g.voff[n_levels]), 16));
+  // plan the levels: separable ones (two launches for all of them), tiled fine
+  // levels (one launch), the rest per vertex with G lanes (runs of equal G)
+  long long hoff = 0, rb = 0, cb = 0, tb = 0;
+  size_t tsmem = 0;
+  int rest[kMaxLevels], nrest = 0;
+  for (int l = 0; l < n_levels; ++l) {
+    if (separable_level(extents, l)) {
+      const int k = g.nsep++;
+      g.sep_l[k] = l;
+      g.sep_gr[k] = lanes_for_terms(double(g.cw0[l]));  // one cell per row item
+      g.sep_gc[k] = lanes_for_terms(2.0 * A / g.E1[l]);
+      g.sep_h[k] = hoff;
+      hoff += (long long)A * g.E0[l];
+      g.sep_rb[k] = rb;
+      rb += ((long long)A * g.E0[l] * g.sep_gr[k] + 255) / 256;
+      g.sep_cb[k] = cb;
+      cb += ((long long)g.E0[l] * g.E1[l] * g.sep_gc[k] + 255) / 256;
+    } else if (lanes_for(l) <= 8 && tile_smem(g, l) <= kTileSmemCap) {
+      const int k = g.ntile++;
+      g.tile_l[k] = l;
+      g.tile_gx[k] = (g.E0[l] + kTX - 1) / kTX;
+      g.tile_b[k] = tb;
+      tb += (long long)g.tile_gx[k] * ((g.E1[l] + kTY - 1) / kTY);
+      tsmem = tile_smem(g, l) > tsmem ? tile_smem(g, l) : tsmem;
     } else {
-      PTY_LANES(G, k_gvert_group, nvv, g, va, vb)
+      rest[nrest++] = l;
     }
-    l0 = l1;
   }
-#undef PTY_LANES
+  g.sep_rb[g.nsep] = rb;
+  g.sep_cb[g.nsep] = cb;
+  g.tile_b[g.ntile] = tb;
+  if (g.nsep) {
+    k_gsep_rows<<<unsigned(rb), 256, 0, s>>>(g);
+    k_gsep_cols<<<unsigned(cb), 256, 0, s>>>(g);
+  }
+  if (g.ntile) {
+    if (tsmem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_gvert_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTileSmemCap)) !=
+            cudaSuccess)
+      return PTYCHO_ERR_LAUNCH;
+    k_gvert_tile<<<unsigned(tb), 256, tsmem, s>>>(g);
+  }
+  for (int r = 0; r < nrest;) {
+    const int l0 = rest[r], G = lanes_for(l0);
+    int r1 = r + 1;
+    while (r1 < nrest && rest[r1] == rest[r1 - 1] + 1 && lanes_for(rest[r1]) == G) ++r1;
+    const long long va = g.voff[l0], vb = g.voff[rest[r1 - 1] + 1], nvv = vb - va;
+    switch (G) {
+      case 256: k_gvert_warp<8><<<unsigned(nvv), 256, 0, s>>>(g, va, vb); break;
+      case 32: k_gvert_group<32><<<unsigned((nvv * 32 + 255) / 256), 256, 0, s>>>(g, va, vb); break;
+      case 16: k_gvert_group<16><<<unsigned((nvv * 16 + 255) / 256), 256, 0, s>>>(g, va, vb); break;
+      case 8: k_gvert_group<8><<<unsigned((nvv * 8 + 255) / 256), 256, 0, s>>>(g, va, vb); break;
+      case 4: k_gvert_group<4><<<unsigned((nvv * 4 + 255) / 256), 256, 0, s>>>(g, va, vb); break;
+      case 2: k_gvert_group<2><<<unsigned((nvv * 2 + 255) / 256), 256, 0, s>>>(g, va, vb); break;
+      default: k_gvert_group<1><<<unsigned((nvv + 255) / 256), 256, 0, s>>>(g, va, vb); break;
+    }
+    r = r1;
+  }
   k_gentry<<<unsigned((L.total + 255) / 256), 256, 0, s>>>(g.vstart, g.vorder, g.G, L.total,
                                                            reinterpret_cast<float2*>(dtable), accumulate);
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;

@@ -243,7 +243,9 @@ class Encoding(torch.nn.Module):
         g = torch.Generator().manual_seed(seed)
         self.params = torch.nn.Parameter(torch.rand(n * 2, generator=g) * 2e-4 - 1e-4)
         self._csr = []
-        self.use_grid_plan = True  # grid coordinates take the CSR-free backward
+        # grid coordinates take the CSR-free backward when it pays ("auto"); True
+        # forces it on grid coordinates, False never uses it
+        self.use_grid_plan = "auto"
 
     def _plan_for(self, coords: torch.Tensor):
         """The backward's static set-up for ``coords``, cached per coordinate
@@ -262,7 +264,7 @@ class Encoding(torch.nn.Module):
                 return plan
         plan = None
         axes = grid_axes(coords) if self.use_grid_plan else None
-        if axes is not None:
+        if axes is not None and (self.use_grid_plan is True or self._grid_pays(axes)):
             try:
                 plan = GridPlan(axes[0], axes[1], self.cfg, self.n_entries).to(coords.device)
                 nbytes = int(_lib.lib().ptycho_hashgrid_grid_scratch_size(plan.hl.ctypes.data, self.n_levels,
@@ -274,6 +276,18 @@ class Encoding(torch.nn.Module):
             plan = _CSR(coords, self.cfg, self.n_entries)
         self._csr = self._csr[-3:] + [(key, coords, coords._version, plan)]
         return plan
+
+    def _grid_pays(self, axes) -> bool:
+        """The vertex-centric grid backward visits every vertex of every level; when
+        the vertices far outnumber the coordinates (a small probe grid under the
+        object's fine levels) the CSR of the few contributions is the better plan."""
+        n = axes[0].size * axes[1].size
+        nvert = 0
+        for lev in level_table(*self.cfg):
+            e0 = int(_axis_cells(axes[0], lev[0])[0].max()) + 2
+            e1 = int(_axis_cells(axes[1], lev[0])[0].max()) + 2
+            nvert += e0 * e1
+        return nvert <= 4 * n
 
     def _csr_for(self, coords: torch.Tensor) -> _CSR:
         """The contribution CSR of ``coords`` (any coordinates), cached like _plan_for."""

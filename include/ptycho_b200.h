@@ -395,9 +395,10 @@ int ptycho_gs_backward(int kind, const float* xy, const float* p1, const float* 
  * coordinates whose cells touch it, then every entry sums its vertices.
  * extents: HOST [n_levels][4] int32 per level: vertex extents E0, E1 and the
  *   most axis values in one cell along each axis (cw0, cw1).  Coarse levels
- *   (cw0 * cw1 >= 16) are summed separably: rows first (H[i][cx] = sum over
- *   the cell pair of wx g), then columns (G = sum over rows of wy H); finer
- *   levels per vertex.
+ *   (cw0 * cw1 >= 16) are summed separably: a row pass forms per row and
+ *   cell S0 = sum (1 - fx) g and S1 = sum fx g, a column pass sums
+ *   wy (S1[cx - 1] + S0[cx]) over the rows of each vertex; finer levels per
+ *   vertex from shared-memory tiles.
  * grid_int (device int32): ix0 [L][Bj], iy1 [L][A] (cell corners of the axis
  *   values), lo0 [sum (E0+1)], lo1 [sum (E1+1)] (first axis index whose corner
  *   is >= c), vstart [entries+1], vorder [vertices] (vertices sorted by entry);
