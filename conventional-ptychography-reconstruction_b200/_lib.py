@@ -122,6 +122,32 @@ def _bind_fast(L) -> None:
     _fast = _fastabi
 
 
+_torchext = None
+_torchext_tried = False
+
+
+def torchext():
+    """The fused loss's C++ autograd node (csrc/torch_ext.cpp) bound to this
+    process's library, or None when it is not built."""
+    global _torchext, _torchext_tried
+    if _torchext_tried:
+        return _torchext
+    L = lib()
+    with _lock:
+        if not _torchext_tried:
+            try:
+                from . import _torchext as m
+            except ImportError:
+                m = None
+            if m is not None:
+                addr = lambda f: ctypes.cast(f, ctypes.c_void_p).value  # noqa: E731
+                m.bind(addr(L.ptycho_fwd_adj), addr(L.ptycho_scale_pair), addr(L.ptycho_fwd_adj_workspace_size),
+                       addr(L.ptycho_status_string))
+            _torchext = m
+            _torchext_tried = True
+    return _torchext
+
+
 def fwd_adj(*args) -> int:
     """ptycho_fwd_adj with the argument list of include/ptycho_b200.h."""
     lib()

@@ -157,6 +157,9 @@ class FwdAdjWorkspace:
 
 
 _default_ws: dict = {}
+# route fused_loss through the C++ autograd node (csrc/torch_ext.cpp) when it
+# is built; False keeps the Python Function (both call the same library)
+USE_TORCHEXT = True
 _ws_size_cache: dict = {}  # (H, W, M, N, B) -> ptycho_fwd_adj_workspace_size
 
 
@@ -232,13 +235,18 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
     ws_bytes = _ws_size_cache.get(key)
     if ws_bytes is None:
         ws_bytes = _ws_size_cache[key] = int(_lib.lib().ptycho_fwd_adj_workspace_size(H, W, M, N, B))
-    if workspace is None:
+    if workspace is not None:
+        ws = workspace.get(ws_bytes, dev)
+    elif USE_TORCHEXT and _lib.torchext() is not None:
+        # the per-stream workspace the C++ autograd node also uses
+        ws = _lib.torchext().workspace(O, ws_bytes)
+    else:
         # one default workspace per (device, stream): calls on one stream are
         # ordered, calls on different streams must not share scratch
         workspace = _default_ws.get((dev, stream))
         if workspace is None:
             workspace = _default_ws.setdefault((dev, stream), FwdAdjWorkspace())
-    ws = workspace.get(ws_bytes, dev)
+        ws = workspace.get(ws_bytes, dev)
     st = device_status(dev)
     _lib.check(_lib.fwd_adj(
         O.data_ptr(), H, W, P.data_ptr(), M, N, tl.data_ptr(), Imeas.data_ptr(), F,
@@ -356,11 +364,21 @@ def fused_loss(object_complex: torch.Tensor, probe_complex: torch.Tensor, tl: to
     frames; ``batch`` [B] frame ids of this minibatch (None: all frames).
     Returns a 0-d float64 tensor; ``backward()`` deposits dO / dP (torch's
     complex convention) into the inputs that require grad."""
-    if loss_type not in LOSS_CODES:
+    code = LOSS_CODES.get(loss_type)
+    if code is None:
         raise ValueError(f"loss_type must be one of {tuple(LOSS_CODES)}, got {loss_type!r}")
     if object_complex.dtype != torch.complex64 or probe_complex.dtype != torch.complex64:
         raise TypeError("object and probe must be complex64")
-    return _FusedLoss.apply(object_complex, probe_complex, tl, Imeas, LOSS_CODES[loss_type], batch)
+    if not object_complex.is_cuda:
+        raise ValueError("object must be a CUDA tensor (there is no CPU path)")
+    ext = _lib.torchext() if USE_TORCHEXT else None
+    if ext is not None:
+        # the C++ autograd node: same library calls, no Python in forward or backward
+        if batch is not None and not isinstance(batch, torch.Tensor):
+            batch = torch.as_tensor(batch)
+        return ext.fused_loss(object_complex, probe_complex, tl, Imeas, code, batch,
+                              device_status(object_complex.device))
+    return _FusedLoss.apply(object_complex, probe_complex, tl, Imeas, code, batch)
 
 
 class _ForwardIntensity(torch.autograd.Function):
