@@ -199,6 +199,79 @@ def parity_vs_cpu(pkg, work, first, dev):
     return out
 
 
+def side_workload(pkg, key, dev, steps=30, warmup=5, n_check=8):
+    """Throughput and parity of the fused path on another workload's shapes
+    (c3 / c4: the 256^2 cluster kernel), run inside the default c1 bench.
+
+    Same object, probe and raster recipe as ``synth.make_workload(key)``; the
+    measurements are generated for 2 x batch frames taken at a regular stride
+    over the whole raster (so minibatches cover the canvas as random ones from
+    the full scan do) and the peak is scaled over those frames.  Steps replay
+    the same CUDA graph as the headline (FwdAdjPlan), L2 flushed before each,
+    CUDA events per step.  Parity: ``n_check`` frames of the first minibatch
+    against the FP64 oracle (intensities, per-pattern losses, dO, dP)."""
+    synth = pkg.synth
+    w = synth.WORKLOADS[key]
+    B, M = w.batch, w.probe
+    O = synth.make_object(w.canvas, seed=0)
+    P = synth.make_probe(w.probe, w.aperture)
+    tlY, tlX = synth.make_scan(w.n_scan, w.step, w.jitter, w.canvas, w.probe, seed=2)
+    stride = max(1, tlY.size // (2 * B))
+    sel = np.arange(0, tlY.size, stride)[:2 * B]
+    tlY, tlX = tlY[sel], tlX[sel]
+    I = synth._intensities(O, P, tlY, tlX, device=dev)
+    I *= w.peak / I.max()
+    Imeas = np.random.default_rng(1).poisson(I).astype(np.float32)
+    del I
+    O, P = O.astype(np.complex64), P.astype(np.complex64)
+    Ot, Pt = torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev)
+    tl = pkg.make_windows(tlY, tlX, dev)
+    stack = torch.from_numpy(Imeas).to(dev)
+    F = tlY.size
+    rng = np.random.default_rng(77)
+    batches = [torch.from_numpy(rng.permutation(F)[:B].astype(np.int32)).to(dev) for _ in range(8)]
+    plan = pkg.optics.FwdAdjPlan(Ot, Pt, tl, stack, w.loss_type, B)
+    plan.capture()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream(dev)
+    for i in range(warmup):
+        plan.batch.copy_(batches[i % 8])
+        plan.replay()
+        flush.zero_()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        plan.batch.copy_(batches[k % 8])
+        flush.zero_()
+        ev[k][0].record(s)
+        plan.replay()
+        ev[k][1].record(s)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    ids = batches[0][:n_check].cpu().numpy()
+    loss, lp, dO, dP = pkg.fwd_adj_raw(Ot, Pt, tl, stack, pkg.LOSS_CODES[w.loss_type],
+                                       batch=batches[0][:n_check].contiguous(), per_pattern=True)
+    Ig = pkg.forward_intensity(Ot, Pt, tl, batch=batches[0][:n_check].contiguous())
+    from oracle import forward_model as fm  # the FP64 NumPy oracle, as the checker
+    ref = fm.fwd_adj(O.astype(np.complex128), P.astype(np.complex128), tlY[ids], tlX[ids], Imeas[ids],
+                     w.loss_type)
+    rn = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())  # noqa: E731
+    bpp = algorithmic_bytes_per_pattern(M, B)
+    return {"workload": f"{key}: {w.canvas}^2 object, {M}^2 probe, batch {B}, {w.loss_type}",
+            "patterns_per_s": B / (ms / 1e3), "ms_per_step": ms, "steps": steps,
+            "hbm_frac_of_measured": bpp * B / (ms / 1e3) / 1e9 / measured_peak_hbm()[0],
+            "frames": f"{F} of the {w.n_scan ** 2} raster positions (every {stride}th)",
+            "parity_vs_fp64_oracle": {
+                "patterns": int(n_check),
+                "intensity_rel_err": rn(Ig.cpu().numpy(), ref["I"]),
+                "loss_per_pattern_max_rel_err": float(np.max(np.abs(lp.cpu().numpy() - ref["loss"])
+                                                             / np.abs(ref["loss"]))),
+                "dO_rel_err": rn(dO.cpu().numpy(), ref["dO"]),
+                "dP_rel_err": rn(dP.cpu().numpy(), ref["dP"])},
+            "note": "one CUDA-graph launch per minibatch (k_fused256 + k_assemble), L2 flushed before "
+                    "each step; clocks not sampled for these steps"}
+
+
 def run_reference(args):
     """--impl reference: the reference's torch CPU path on this host's cores."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -460,6 +533,16 @@ def run_ours(args):
                 "clocks": clk.summary(note=f"sampled every 50 ms over the {args.steps} timed steps and "
                                            f"{n_settle} identical untimed steps on either side "
                                            f"(~{SETTLE_S:.1f} s each)")}
+        if world == 1 and not args.no_side and args.workload == "c1":
+            # the 256^2 cluster path on the c3 / c4 shapes, recorded beside the headline
+            side = {}
+            for key in ("c3", "c4"):
+                try:
+                    side[key] = side_workload(pkg, key, dev)
+                except Exception as exc:  # reported, not fatal for the throughput line
+                    side[key] = {"error": f"{type(exc).__name__}: {exc}"}
+                torch.cuda.empty_cache()
+            line["other_workloads"] = side
         if world == 1 and not args.no_ttr and args.workload == "c1":
             # the headline's second half: time-to-residual, INR vs pixel grid (c2); run
             # before the CPU baseline, whose idle OpenMP workers would share the host
@@ -968,6 +1051,7 @@ def main():
     ap.add_argument("--inr-cap-s", type=float, default=60.0)
     ap.add_argument("--ref-cap-s", type=float, default=90.0)
     ap.add_argument("--no-ttr", action="store_true", help="omit the time-to-residual object from the bench line")
+    ap.add_argument("--no-side", action="store_true", help="omit the c3 / c4 records from the c1 bench line")
     ap.add_argument("--gs", action="store_true", help="time the Gaussian-field rasteriser instead")
     ap.add_argument("--c0-reconstruction", action="store_true",
                     help="run workload c0's full pixel-grid reconstruction on the GPU and the CPU reference loop")
