@@ -9,7 +9,7 @@
 namespace pty {
 
 struct WsLayout {
-  size_t E, scr, part, loss, tlb, done, total;
+  size_t E, scr, part, loss, tlb, done, lpart, total;
 };
 
 // square 64, 128, 256: the fused kernels; every other M x N: the general path
@@ -32,6 +32,8 @@ static WsLayout ws_layout(int M, int N, int B) {
   off += pty_align_up(size_t(B) * sizeof(int2), 256);
   L.done = off;  // arrival counters of the dP reduction (self-resetting)
   off += pty_align_up(size_t(dp_counters(M, N)) * sizeof(unsigned), 256);
+  L.lpart = off;  // M = 256 line-DFT path: FP64 loss partial per (pattern, column block)
+  if (M == 256 && N == 256) off += pty_align_up(size_t(B) * kSplit256Blocks * sizeof(double), 256);
   L.total = off;
   return L;
 }
@@ -171,14 +173,24 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   a.loss_pat = lp;
   const bool adj = dO || dP;
   const bool fused = fused_probe(M, N);
-  if (fused) {
+  const int mode = adj ? MODE_ADJ : MODE_LOSS;
+  if (fused && M == 256 && split256_supported(mode, loss_type)) {
+    // the line-DFT kernels use E' as their scratch in both modes
+    a.Eout = Ews;
+    a.tlb = tlb;
+    if (adj) {
+      a.done = done;
+      a.ndone = dp_counters(M, N);
+    }
+    st = launch_split256(mode, loss_type, a, reinterpret_cast<double*>(ws + L.lpart), s);
+  } else if (fused) {
     if (adj) {
       a.Eout = Ews;
       a.tlb = tlb;
       a.done = done;
       a.ndone = dp_counters(M, N);
     }
-    st = launch_fused(M, adj ? MODE_ADJ : MODE_LOSS, loss_type, a, s);
+    st = launch_fused(M, mode, loss_type, a, s);
   } else {
     // the arrival counters start at zero: the fused kernel zeroes them, here a memset
     if (adj && cudaMemsetAsync(done, 0, size_t(dp_counters(M, N)) * sizeof(unsigned), s) != cudaSuccess)

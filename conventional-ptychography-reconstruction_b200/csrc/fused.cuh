@@ -368,4 +368,11 @@ int launch_fused_64(int mode, int loss, const FusedArgs& a, cudaStream_t s);
 int launch_fused_128(int mode, int loss, const FusedArgs& a, cudaStream_t s);
 int launch_fused_256(int mode, int loss, const FusedArgs& a, cudaStream_t s);
 
+// split256.cu: M = 256 as three line-DFT kernels (smooth-L1, Poisson and the
+// intensity-gradient losses in MODE_LOSS / MODE_ADJ); a.Eout is the scratch,
+// lpart holds B * kSplit256Blocks doubles
+constexpr int kSplit256Blocks = 16;
+bool split256_supported(int mode, int loss);
+int launch_split256(int mode, int loss, const FusedArgs& a, double* lpart, cudaStream_t s);
+
 }  // namespace pty

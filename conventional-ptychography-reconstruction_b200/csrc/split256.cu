@@ -1,0 +1,359 @@
+// split256.cu -- forward / loss / adjoint for 256 x 256 probes as three
+// line-DFT kernels over the E' workspace (smooth-L1, Poisson and the
+// intensity-gradient losses; the FD loss and MODE_INTENSITY keep the
+// cluster kernel of fused256.cu).
+//
+// Same contract as the fused kernels (fused.cuh): per pattern b of the batch,
+//   A  rows:     X_b[y][.] = DFT_x( (-1)^(x+y) P[y][x] O[tlY+y][tlX+x] )
+//   B  columns:  F_b[.][fx] = DFT_y(X_b[.][fx])   (= fftshift(fft2(P * O_w)))
+//                loss terms against Imeas[f_b] at the same index (the sign
+//                folds fftshift in), FP64 partial per column block;
+//                G = 2 dL/dI F;  X_b[.][fx] = IDFT_y(G[.][fx])  (unnormalised)
+//   C  rows:     E'_b[y][.] = IDFT_x(X_b[y][.]); per-pattern loss from the
+//                column-block partials in a fixed order
+// so E'_b = (-1)^(x+y) dL/dpsi_b, the layout the assembly (assemble.cu)
+// reads.  X_b is E'_b's own workspace slot: no other scratch.  Patterns run
+// in chunks of kChunk so a chunk's slots stay in L2 between the three
+// kernels.
+//
+// Line DFT of length 256 = 16 x 16 on a half-warp: lane j holds the values
+// j + 16 k (k = 0..15) in registers; a 16-point DFT over k, the twiddle
+// W256^(j p), a 16 x 16 transpose through shared memory (padded rows of 17:
+// both half-warps of a warp hit disjoint banks), a second 16-point DFT.
+// Lane p then holds the outputs p + 16 q -- the input layout -- so lines
+// chain without reordering.  Everything is a fixed sequence: results are
+// bitwise deterministic.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dft_regs.cuh"
+#include "fused.cuh"
+
+#ifndef PTY_S256_CHUNK
+#define PTY_S256_CHUNK 64
+#endif
+
+namespace pty {
+namespace s256 {
+
+constexpr int M = 256;
+constexpr int NT = 256;            // 16 lines x 16 lanes per CTA
+constexpr int LINES = 16;
+constexpr int TP = 17;             // padded row of a 16 x 16 transpose / tile
+constexpr int BUF = LINES * 16 * TP;  // floats per plane (re or im): 4352
+constexpr int NCB = M / LINES;     // column (or row) blocks per pattern: 16
+static_assert(NCB == kSplit256Blocks, "loss partials per pattern");
+constexpr int kChunk = PTY_S256_CHUNK;
+
+// shared memory: twiddles, two planes (tile / transposes), measurement tile, reduction
+constexpr size_t SM_TW = 0;
+constexpr size_t SM_RE = SM_TW + M * 8;
+constexpr size_t SM_IM = SM_RE + BUF * 4;
+constexpr size_t SM_MEAS = SM_IM + BUF * 4;
+constexpr size_t SM_RED = SM_MEAS + size_t(M) * TP * 4;
+constexpr size_t SMEM_ROWS = SM_MEAS;             // kernels A and C
+constexpr size_t SMEM_COLS = SM_RED + 8 * 8;      // kernel B
+
+struct Args {
+  FusedArgs f;
+  double* lpart;  // [B][NCB] FP64 loss partial of each column block
+  int b0;         // first pattern of this chunk
+};
+
+// W256^k, k = 0..255 (forward sign), one entry per thread
+PTY_DEVI void fill_twiddles(float2* tw) {
+  float s, c;
+  sincospif(-float(threadIdx.x) / 128.0f, &s, &c);
+  tw[threadIdx.x] = make_float2(c, s);
+}
+
+// 256-point DFT (INV: unnormalised inverse) of one line held by a half-warp.
+// In: lane j holds x[j + 16 k] in v[k].  Out: lane j holds X[j + 16 q] in v[q].
+// bre / bim: this line's private 16 x 17 transpose planes.
+template <bool INV>
+PTY_DEVI void line256(float2 (&v)[16], int j, float* bre, float* bim, const float2* tw) {
+  dft16<INV, 1>(v);  // v[p] = sum_k x[j + 16 k] W16^(k p)
+#pragma unroll
+  for (int p = 1; p < 16; ++p) {
+    const float2 w = tw[(j * p) & (M - 1)];
+    v[p] = c_mul(v[p], INV ? c_conj(w) : w);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int p = 0; p < 16; ++p) {
+    bre[p * TP + j] = v[p].x;
+    bim[p * TP + j] = v[p].y;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = make_float2(bre[j * TP + i], bim[j * TP + i]);
+  dft16<INV, 1>(v);  // v[q] = X[j + 16 q]
+}
+
+PTY_DEVI bool window_ok(const FusedArgs& a, int b, int& f, int2& w) {
+  f = a.batch ? __ldg(a.batch + b) : b;
+  if (f < 0 || f >= a.F) {
+    w = make_int2(-1, -1);
+    return false;
+  }
+  w = __ldg(a.tl + f);
+  return w.x >= 0 && w.y >= 0 && w.x <= a.H - M && w.y <= a.W - M;
+}
+
+// A: gather + row DFTs.  grid (NCB, chunk): CTA (rb, b - b0) owns rows
+// 16 rb .. 16 rb + 15 of pattern b.  Also resolves the window (tlb, status)
+// and, once per call, zeroes the assembly's dP arrival counters.
+__global__ void __launch_bounds__(NT, 4) k_rows_fwd(const Args g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
+  float* pre = reinterpret_cast<float*>(smem + SM_RE);
+  float* pim = reinterpret_cast<float*>(smem + SM_IM);
+  const FusedArgs& a = g.f;
+  const int t = threadIdx.x, r = t >> 4, j = t & 15;
+  const int b = g.b0 + blockIdx.y;
+  const int y = blockIdx.x * LINES + r;
+  if (g.b0 == 0 && blockIdx.x == 0 && blockIdx.y == 0 && a.done)
+    for (int i = t; i < a.ndone; i += NT) a.done[i] = 0u;
+  int f;
+  int2 w;
+  const bool ok = window_ok(a, b, f, w);
+  if (blockIdx.x == 0 && t == 0) {
+    a.tlb[b] = ok ? w : make_int2(-1, -1);
+    if (!ok) pty_raise(a.status, PTYCHO_ERR_WINDOW);
+  }
+  if (!ok) return;  // uniform over the CTA
+  fill_twiddles(tw);
+  float2 v[16];
+  {
+    const float2* Or = a.O + size_t(w.x + y) * a.W + w.y + j;
+    const float2* Pr = a.P + y * M + j;
+    const unsigned sg = unsigned((j + y) & 1) << 31;  // (-1)^(x+y), x = j + 16 k
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      float2 pv = __ldg(Pr + 16 * k);
+      pv.x = __uint_as_float(__float_as_uint(pv.x) ^ sg);
+      pv.y = __uint_as_float(__float_as_uint(pv.y) ^ sg);
+      v[k] = c_mul(pv, __ldg(Or + 16 * k));
+    }
+  }
+  __syncthreads();  // twiddles ready
+  line256<false>(v, j, pre + r * 16 * TP, pim + r * 16 * TP, tw);
+  float2* Xr = a.Eout + size_t(b) * M * M + size_t(y) * M + j;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) Xr[16 * q] = v[q];
+}
+
+// C: inverse row DFTs in place -> E'.  grid (NCB, chunk).  CTA (0, b)
+// also writes the pattern's loss: its NCB column-block partials summed in
+// order, / M^2 (NaN for a skipped window).
+__global__ void __launch_bounds__(NT, 4) k_rows_inv(const Args g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
+  float* pre = reinterpret_cast<float*>(smem + SM_RE);
+  float* pim = reinterpret_cast<float*>(smem + SM_IM);
+  const FusedArgs& a = g.f;
+  const int t = threadIdx.x, r = t >> 4, j = t & 15;
+  const int b = g.b0 + blockIdx.y;
+  const int y = blockIdx.x * LINES + r;
+  const bool ok = __ldg(&a.tlb[b].x) >= 0;
+  if (blockIdx.x == 0 && t == 0 && a.loss_pat) {
+    double s = 0.0;
+    for (int cb = 0; cb < NCB; ++cb) s += g.lpart[size_t(b) * NCB + cb];
+    a.loss_pat[b] = ok ? s / double(M * M) : (double)__int_as_float(0x7fc00000);
+  }
+  if (!ok) return;
+  fill_twiddles(tw);
+  float2* Xr = a.Eout + size_t(b) * M * M + size_t(y) * M + j;
+  float2 v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = Xr[16 * k];
+  __syncthreads();
+  line256<true>(v, j, pre + r * 16 * TP, pim + r * 16 * TP, tw);
+#pragma unroll
+  for (int q = 0; q < 16; ++q) Xr[16 * q] = v[q];
+}
+
+// B: column DFTs, loss, and (GRAD) the gradient's inverse column DFTs.
+// grid (NCB, chunk): CTA (cb, b - b0) owns columns 16 cb .. 16 cb + 15 of
+// pattern b; the 256 x 16 tile and the measurement's 256 x 16 block come in
+// through shared memory as 16-byte row pieces.
+template <int LOSS, bool GRAD>
+__global__ void __launch_bounds__(NT, 4) k_cols(const Args g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
+  float* pre = reinterpret_cast<float*>(smem + SM_RE);
+  float* pim = reinterpret_cast<float*>(smem + SM_IM);
+  float* msm = reinterpret_cast<float*>(smem + SM_MEAS);
+  double* red = reinterpret_cast<double*>(smem + SM_RED);
+  const FusedArgs& a = g.f;
+  const int t = threadIdx.x, c = t >> 4, j = t & 15;
+  const int b = g.b0 + blockIdx.y;
+  const int fx0 = blockIdx.x * LINES;
+  if (__ldg(&a.tlb[b].x) < 0) return;  // skipped window (uniform)
+  const int f = a.batch ? __ldg(a.batch + b) : b;
+  float2* Xb = a.Eout + size_t(b) * M * M + fx0;
+  {
+    // measurement rows fy: 16 floats at fx0 (four 16-byte pieces per row)
+    const float* Ib = a.Imeas + size_t(f) * M * M + fx0;
+    float4 mv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = t + NT * k;
+      mv[k] = __ldg(reinterpret_cast<const float4*>(Ib + size_t(i >> 2) * M) + (i & 3));
+    }
+    float4 xv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = t + NT * k;
+      xv[k] = *(reinterpret_cast<const float4*>(Xb + size_t(i >> 3) * M) + (i & 7));
+    }
+    fill_twiddles(tw);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = t + NT * k;
+      float* d = msm + (i >> 2) * TP + 4 * (i & 3);
+      d[0] = mv[k].x;
+      d[1] = mv[k].y;
+      d[2] = mv[k].z;
+      d[3] = mv[k].w;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = t + NT * k;
+      const int o = (i >> 3) * TP + 2 * (i & 7);
+      pre[o] = xv[k].x;
+      pim[o] = xv[k].y;
+      pre[o + 1] = xv[k].z;
+      pim[o + 1] = xv[k].w;
+    }
+  }
+  __syncthreads();
+  float2 v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = make_float2(pre[(j + 16 * k) * TP + c], pim[(j + 16 * k) * TP + c]);
+  __syncthreads();  // the tile region becomes the lines' transpose planes
+  float* bre = pre + c * 16 * TP;
+  float* bim = pim + c * 16 * TP;
+  line256<false>(v, j, bre, bim, tw);  // v[q] = F[j + 16 q][fx0 + c]
+
+  constexpr float inv_mn = 1.0f / float(M * M);
+  float part[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const float meas = msm[(j + 16 * q) * TP + c];
+    const float I = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
+    if constexpr (LOSS == PTYCHO_LOSS_INTENSITY_GRAD) {
+      part[q] = I * meas * float(M * M);
+      v[q] = c_scale(v[q], 2.0f * meas);
+    } else {
+      float gq;
+      if constexpr (LOSS == PTYCHO_LOSS_SMOOTH_L1) {
+        const float dd = I - meas;
+        const float ad = fabsf(dd);
+        part[q] = ad < 1.0f ? 0.5f * dd * dd : ad - 0.5f;
+        gq = ad < 1.0f ? dd : copysignf(1.0f, dd);
+      } else {
+        const float Ie = I + kEps;
+        part[q] = fmaf(-meas, __logf(Ie), I);
+        gq = 1.0f - __fdividef(meas, Ie);
+      }
+      v[q] = c_scale(v[q], 2.0f * gq * inv_mn);
+    }
+  }
+#pragma unroll
+  for (int w = 1; w < 16; w <<= 1)
+#pragma unroll
+    for (int i = 0; i < 16; i += 2 * w) part[i] += part[i + w];
+  const double tot = block_sum<NT>((double)part[0], red);
+  if (t == 0) g.lpart[size_t(b) * NCB + blockIdx.x] = tot;
+  if constexpr (GRAD) {
+    line256<true>(v, j, bre, bim, tw);  // v[q] = X2[j + 16 q][fx0 + c]
+    __syncthreads();  // every line is done with its transpose planes
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      pre[(j + 16 * q) * TP + c] = v[q].x;
+      pim[(j + 16 * q) * TP + c] = v[q].y;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = t + NT * k;
+      const int o = (i >> 3) * TP + 2 * (i & 7);
+      *(reinterpret_cast<float4*>(Xb + size_t(i >> 3) * M) + (i & 7)) =
+          make_float4(pre[o], pim[o], pre[o + 1], pim[o + 1]);
+    }
+  }
+}
+
+// MODE_LOSS: per-pattern losses from the column-block partials (fixed order)
+__global__ void k_loss_pat(const Args g) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= g.f.B || !g.f.loss_pat) return;
+  const bool ok = g.f.tlb[b].x >= 0;
+  double s = 0.0;
+  for (int cb = 0; cb < NCB; ++cb) s += g.lpart[size_t(b) * NCB + cb];
+  g.f.loss_pat[b] = ok ? s / double(M * M) : (double)__int_as_float(0x7fc00000);
+}
+
+template <typename K>
+static bool set_smem(K kern, size_t bytes, PtyDevCache& cache) {
+  int dev;
+  if (cache.get(&dev)) return true;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) != cudaSuccess)
+    return false;
+  cache.put(dev, 1);
+  return true;
+}
+
+template <int LOSS>
+static int launch_t(bool adj, const FusedArgs& fa, double* lpart, cudaStream_t s) {
+  // "shared-memory attribute set" per device and kernel; cleared when a
+  // launch is refused (a device reset drops the attribute), so the next
+  // call sets it again
+  static PtyDevCache c_rows_fwd, c_rows_inv, c_cols_adj, c_cols_loss;
+  PtyDevCache& c_cols = adj ? c_cols_adj : c_cols_loss;
+  auto kcols = adj ? k_cols<LOSS, true> : k_cols<LOSS, false>;
+  if (!set_smem(k_rows_fwd, SMEM_ROWS, c_rows_fwd) || !set_smem(k_rows_inv, SMEM_ROWS, c_rows_inv) ||
+      !set_smem(kcols, SMEM_COLS, c_cols))
+    return PTYCHO_ERR_LAUNCH;
+  Args g{fa, lpart, 0};
+  for (int b0 = 0; b0 < fa.B; b0 += kChunk) {
+    const int n = fa.B - b0 < kChunk ? fa.B - b0 : kChunk;
+    g.b0 = b0;
+    const dim3 grid(NCB, n);
+    k_rows_fwd<<<grid, NT, SMEM_ROWS, s>>>(g);
+    kcols<<<grid, NT, SMEM_COLS, s>>>(g);
+    if (adj) k_rows_inv<<<grid, NT, SMEM_ROWS, s>>>(g);
+  }
+  if (!adj) k_loss_pat<<<(fa.B + 255) / 256, 256, 0, s>>>(g);
+  if (cudaGetLastError() == cudaSuccess) return PTYCHO_OK;
+  int dev;
+  for (PtyDevCache* c : {&c_rows_fwd, &c_rows_inv, &c_cols})
+    if (c->get(&dev)) c->put(dev, 0);
+  return PTYCHO_ERR_LAUNCH;
+}
+
+}  // namespace s256
+}  // namespace pty
+
+namespace pty {
+
+bool split256_supported(int mode, int loss) {
+  return (mode == MODE_LOSS || mode == MODE_ADJ) &&
+         (loss == PTYCHO_LOSS_SMOOTH_L1 || loss == PTYCHO_LOSS_POISSON || loss == PTYCHO_LOSS_INTENSITY_GRAD);
+}
+
+// a.Eout (B M^2 complex64) is the scratch and, in MODE_ADJ, the output E';
+// a.tlb receives the resolved windows in both modes; lpart holds B * 16 doubles
+int launch_split256(int mode, int loss, const FusedArgs& a, double* lpart, cudaStream_t s) {
+  using namespace s256;
+  if (!split256_supported(mode, loss) || !a.Eout || !a.tlb || !lpart) return PTYCHO_ERR_INVALID_ARG;
+  const bool adj = mode == MODE_ADJ;
+  switch (loss) {
+    case PTYCHO_LOSS_SMOOTH_L1: return launch_t<PTYCHO_LOSS_SMOOTH_L1>(adj, a, lpart, s);
+    case PTYCHO_LOSS_POISSON: return launch_t<PTYCHO_LOSS_POISSON>(adj, a, lpart, s);
+    default: return launch_t<PTYCHO_LOSS_INTENSITY_GRAD>(adj, a, lpart, s);
+  }
+}
+
+}  // namespace pty
