@@ -375,7 +375,7 @@ def run_ours(args):
     # so the clock record spans them plus SETTLE_S of identical untimed steps
     # on either side (same kernels, same flushes).  The count is agreed over
     # ranks, so every rank takes the same collective steps.
-    n_settle = int(min(20000, max(1, SETTLE_S * 1e3 / max(w0.elapsed_time(w1) / max(args.warmup, 1), 1e-3))))
+    n_settle = int(min(20000, max(1, args.settle_s * 1e3 / max(w0.elapsed_time(w1) / max(args.warmup, 1), 1e-3))))
     if world > 1:
         import torch.distributed as dist
         nt = torch.tensor([n_settle], dtype=torch.int64, device=dev)
@@ -532,7 +532,7 @@ def run_ours(args):
                              "full_band_all_reduce_bytes": 8 * (exchange.rows[1] - exchange.rows[0]) * W + 8 * M * M},
                 "clocks": clk.summary(note=f"sampled every 50 ms over the {args.steps} timed steps and "
                                            f"{n_settle} identical untimed steps on either side "
-                                           f"(~{SETTLE_S:.1f} s each)")}
+                                           f"(~{args.settle_s:.1f} s each)")}
         if world == 1 and not args.no_side and args.workload == "c1":
             # the 256^2 cluster path on the c3 / c4 shapes, recorded beside the headline
             side = {}
@@ -1052,6 +1052,8 @@ def main():
     ap.add_argument("--ref-cap-s", type=float, default=90.0)
     ap.add_argument("--no-ttr", action="store_true", help="omit the time-to-residual object from the bench line")
     ap.add_argument("--no-side", action="store_true", help="omit the c3 / c4 records from the c1 bench line")
+    ap.add_argument("--settle-s", type=float, default=SETTLE_S,
+                    help="seconds of untimed steps on either side of the timed ones (clock sampling)")
     ap.add_argument("--gs", action="store_true", help="time the Gaussian-field rasteriser instead")
     ap.add_argument("--c0-reconstruction", action="store_true",
                     help="run workload c0's full pixel-grid reconstruction on the GPU and the CPU reference loop")

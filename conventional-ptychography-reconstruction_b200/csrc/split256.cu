@@ -16,13 +16,16 @@
 // in chunks of kChunk so a chunk's slots stay in L2 between the three
 // kernels.
 //
-// Line DFT of length 256 = 16 x 16 on a half-warp: lane j holds the values
-// j + 16 k (k = 0..15) in registers; a 16-point DFT over k, the twiddle
+// Line DFT of length 256 = 16 x 16.  Rows: a half-warp per row, lane j
+// holding x[j + 16 k] in registers; a 16-point DFT over k, the twiddle
 // W256^(j p), a 16 x 16 transpose through shared memory (padded rows of 17:
-// both half-warps of a warp hit disjoint banks), a second 16-point DFT.
-// Lane p then holds the outputs p + 16 q -- the input layout -- so lines
-// chain without reordering.  Everything is a fixed sequence: results are
-// bitwise deterministic.
+// the two half-warps of a warp hit disjoint banks), a second 16-point DFT;
+// lane p then holds X[p + 16 q], the input layout, so lines chain without
+// reordering.  Columns: the same factorisation with the 16 values of a
+// column spread over 16 half-warps (a half-warp = 16 adjacent columns, so
+// every global access is a 64- or 128-byte row piece) and the transpose
+// across warps.  Everything is a fixed sequence: results are bitwise
+// deterministic.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -31,6 +34,9 @@
 
 #ifndef PTY_S256_CHUNK
 #define PTY_S256_CHUNK 64
+#endif
+#ifndef PTY_S256_COLS_MINB
+#define PTY_S256_COLS_MINB 4
 #endif
 
 namespace pty {
@@ -45,13 +51,12 @@ constexpr int NCB = M / LINES;     // column (or row) blocks per pattern: 16
 static_assert(NCB == kSplit256Blocks, "loss partials per pattern");
 constexpr int kChunk = PTY_S256_CHUNK;
 
-// shared memory: twiddles, two planes (tile / transposes), measurement tile, reduction
+// shared memory: twiddles, two transpose planes (re, im), reduction
 constexpr size_t SM_TW = 0;
 constexpr size_t SM_RE = SM_TW + M * 8;
 constexpr size_t SM_IM = SM_RE + BUF * 4;
-constexpr size_t SM_MEAS = SM_IM + BUF * 4;
-constexpr size_t SM_RED = SM_MEAS + size_t(M) * TP * 4;
-constexpr size_t SMEM_ROWS = SM_MEAS;             // kernels A and C
+constexpr size_t SM_RED = SM_IM + BUF * 4;
+constexpr size_t SMEM_ROWS = SM_RED;              // kernels A and C
 constexpr size_t SMEM_COLS = SM_RED + 8 * 8;      // kernel B
 
 struct Args {
@@ -173,74 +178,70 @@ __global__ void __launch_bounds__(NT, 4) k_rows_inv(const Args g) {
   for (int q = 0; q < 16; ++q) Xr[16 * q] = v[q];
 }
 
+// 256-point DFT of one column per thread slot, spread over the CTA: thread
+// (j, c) = (t >> 4, t & 15) holds x[j + 16 k] of column c in v[k]; a 16-point
+// DFT over k, the twiddle W256^(j p), a transpose across warps through the
+// planes (row p of the transpose at p * CT, so the two half-warps of a warp
+// hit disjoint banks when writing and when reading), a second 16-point DFT.
+// Thread (p, c) then holds X[p + 16 q] in v[q] -- the input layout again.
+// Contains two barriers: every thread of the CTA calls it, with the twiddle
+// table already published by a barrier.
+constexpr int CT = 16 * 16 + 16;  // floats per transpose row p (16 j x 16 c + pad)
+template <bool INV>
+PTY_DEVI void col256(float2 (&v)[16], int j, int c, float* bre, float* bim, const float2* tw) {
+  dft16<INV, 1>(v);
+#pragma unroll
+  for (int p = 1; p < 16; ++p) {
+    const float2 w = tw[(j * p) & (M - 1)];
+    v[p] = c_mul(v[p], INV ? c_conj(w) : w);
+  }
+  __syncthreads();  // earlier readers of the planes are done
+#pragma unroll
+  for (int p = 0; p < 16; ++p) {
+    bre[p * CT + j * 16 + c] = v[p].x;
+    bim[p * CT + j * 16 + c] = v[p].y;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = make_float2(bre[j * CT + i * 16 + c], bim[j * CT + i * 16 + c]);
+  dft16<INV, 1>(v);
+}
+static_assert(16 * CT <= BUF, "column transpose planes fit the plane size");
+
 // B: column DFTs, loss, and (GRAD) the gradient's inverse column DFTs.
 // grid (NCB, chunk): CTA (cb, b - b0) owns columns 16 cb .. 16 cb + 15 of
-// pattern b; the 256 x 16 tile and the measurement's 256 x 16 block come in
-// through shared memory as 16-byte row pieces.
+// pattern b.  Thread (j, c) reads rows j + 16 k of column c: a half-warp
+// reads 16 adjacent columns of one row (128 bytes), and so for the
+// measurement (64 bytes) and the write-back.
 template <int LOSS, bool GRAD>
-__global__ void __launch_bounds__(NT, 4) k_cols(const Args g) {
+__global__ void __launch_bounds__(NT, PTY_S256_COLS_MINB) k_cols(const Args g) {
   extern __shared__ __align__(16) unsigned char smem[];
   float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
-  float* pre = reinterpret_cast<float*>(smem + SM_RE);
-  float* pim = reinterpret_cast<float*>(smem + SM_IM);
-  float* msm = reinterpret_cast<float*>(smem + SM_MEAS);
+  float* bre = reinterpret_cast<float*>(smem + SM_RE);
+  float* bim = reinterpret_cast<float*>(smem + SM_IM);
   double* red = reinterpret_cast<double*>(smem + SM_RED);
   const FusedArgs& a = g.f;
-  const int t = threadIdx.x, c = t >> 4, j = t & 15;
+  const int t = threadIdx.x, j = t >> 4, c = t & 15;
   const int b = g.b0 + blockIdx.y;
   const int fx0 = blockIdx.x * LINES;
   if (__ldg(&a.tlb[b].x) < 0) return;  // skipped window (uniform)
   const int f = a.batch ? __ldg(a.batch + b) : b;
-  float2* Xb = a.Eout + size_t(b) * M * M + fx0;
-  {
-    // measurement rows fy: 16 floats at fx0 (four 16-byte pieces per row)
-    const float* Ib = a.Imeas + size_t(f) * M * M + fx0;
-    float4 mv[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int i = t + NT * k;
-      mv[k] = __ldg(reinterpret_cast<const float4*>(Ib + size_t(i >> 2) * M) + (i & 3));
-    }
-    float4 xv[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int i = t + NT * k;
-      xv[k] = *(reinterpret_cast<const float4*>(Xb + size_t(i >> 3) * M) + (i & 7));
-    }
-    fill_twiddles(tw);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int i = t + NT * k;
-      float* d = msm + (i >> 2) * TP + 4 * (i & 3);
-      d[0] = mv[k].x;
-      d[1] = mv[k].y;
-      d[2] = mv[k].z;
-      d[3] = mv[k].w;
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int i = t + NT * k;
-      const int o = (i >> 3) * TP + 2 * (i & 7);
-      pre[o] = xv[k].x;
-      pim[o] = xv[k].y;
-      pre[o + 1] = xv[k].z;
-      pim[o + 1] = xv[k].w;
-    }
-  }
-  __syncthreads();
+  float2* Xc = a.Eout + size_t(b) * M * M + fx0 + c;
+  const float* Ic = a.Imeas + size_t(f) * M * M + fx0 + c;
+  // the measurement block (256 rows x 64 bytes) towards L2 while the DFT runs
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(Ic - c + size_t(t) * M));
+  fill_twiddles(tw);
   float2 v[16];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = make_float2(pre[(j + 16 * k) * TP + c], pim[(j + 16 * k) * TP + c]);
-  __syncthreads();  // the tile region becomes the lines' transpose planes
-  float* bre = pre + c * 16 * TP;
-  float* bim = pim + c * 16 * TP;
-  line256<false>(v, j, bre, bim, tw);  // v[q] = F[j + 16 q][fx0 + c]
+  for (int k = 0; k < 16; ++k) v[k] = Xc[size_t(j + 16 * k) * M];
+  __syncthreads();  // twiddles ready
+  col256<false>(v, j, c, bre, bim, tw);  // v[q] = F[j + 16 q][fx0 + c]
 
   constexpr float inv_mn = 1.0f / float(M * M);
   float part[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
-    const float meas = msm[(j + 16 * q) * TP + c];
+    const float meas = __ldg(Ic + size_t(j + 16 * q) * M);
     const float I = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
     if constexpr (LOSS == PTYCHO_LOSS_INTENSITY_GRAD) {
       part[q] = I * meas * float(M * M);
@@ -267,21 +268,9 @@ __global__ void __launch_bounds__(NT, 4) k_cols(const Args g) {
   const double tot = block_sum<NT>((double)part[0], red);
   if (t == 0) g.lpart[size_t(b) * NCB + blockIdx.x] = tot;
   if constexpr (GRAD) {
-    line256<true>(v, j, bre, bim, tw);  // v[q] = X2[j + 16 q][fx0 + c]
-    __syncthreads();  // every line is done with its transpose planes
+    col256<true>(v, j, c, bre, bim, tw);  // v[q] = X2[j + 16 q][fx0 + c]
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      pre[(j + 16 * q) * TP + c] = v[q].x;
-      pim[(j + 16 * q) * TP + c] = v[q].y;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int i = t + NT * k;
-      const int o = (i >> 3) * TP + 2 * (i & 7);
-      *(reinterpret_cast<float4*>(Xb + size_t(i >> 3) * M) + (i & 7)) =
-          make_float4(pre[o], pim[o], pre[o + 1], pim[o + 1]);
-    }
+    for (int q = 0; q < 16; ++q) Xc[size_t(j + 16 * q) * M] = v[q];
   }
 }
 

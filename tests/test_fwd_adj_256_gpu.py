@@ -1,5 +1,7 @@
-"""Parity of the 256 x 256 probe path (one 4-CTA cluster per pattern, the
-pass-2/pass-3 exchange through distributed shared memory) with the FP64 oracle.
+"""Parity of the 256 x 256 probe paths with the FP64 oracle: the line-DFT
+kernels (smooth-L1, Poisson and the intensity gradient; patterns in chunks of
+64) and the 4-CTA cluster kernel (FD loss and forward intensities; the
+pass-2/pass-3 exchange through distributed shared memory).
 
 Tolerances as for 64 / 128 (FP32 FFT against FP64):
   forward intensities  max|I - I_ref| / max|I_ref|      <= 1e-5
@@ -100,3 +102,63 @@ def test_fd_loss_only_256(pkg):
                                      pkg.LOSS_CODES["FD_loss"], want_grad=False, per_pattern=True)
     r = fm.fwd_adj(O, P, tlY, tlX, Imeas, "FD_loss")
     assert np.all(np.abs(lp.cpu().numpy() - r["loss"]) <= 2e-5 * np.abs(r["loss"]))
+
+
+def _intensity_grad_ref(O, P, tlY, tlX, gI):
+    """dO, dP of sum(I * gI) in FP64 (the intensity-gradient call's contract)."""
+    O, P = O.astype(np.complex128), P.astype(np.complex128)
+    F = fm.far_field(fm.exit_waves(O, P, tlY, tlX))
+    E = (M * M) * np.fft.ifft2(np.fft.ifftshift(2.0 * gI * F, axes=(-2, -1)), axes=(-2, -1))
+    dO, dP = np.zeros_like(O), np.zeros_like(P)
+    for b in range(tlY.size):
+        y, x = int(tlY[b]), int(tlX[b])
+        dP += E[b] * np.conj(O[y:y + M, x:x + M])
+        dO[y:y + M, x:x + M] += E[b] * np.conj(P)
+    return dO, dP
+
+
+def test_chunks_repeats_and_a_skipped_window_256(pkg):
+    """150 patterns = chunks of 64, 64 and 22; frame ids repeat; one window in
+    the last chunk leaves the canvas (NaN loss, status 6, no contribution);
+    bitwise repeatable."""
+    dev = torch.device("cuda")
+    H, F = 460, 40
+    O, P, tlY, tlX, Imeas = _case(M, H, F, seed=150)
+    ids = np.random.default_rng(3).integers(0, F, 150).astype(np.int32)
+    bad = tlX.copy()
+    bad[ids[140]] = H - M + 3
+    Ot, Pt = torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev)
+    tl = pkg.make_windows(tlY, bad, dev)
+    Im = torch.from_numpy(Imeas).to(dev)
+    bt = torch.from_numpy(ids).to(dev)
+    pkg.read_status(dev, reset=True)
+    runs = [pkg.fwd_adj_raw(Ot, Pt, tl, Im, pkg.LOSS_CODES["Poisson_likelihood_loss"], batch=bt, per_pattern=True)
+            for _ in range(2)]
+    torch.cuda.synchronize()
+    assert pkg.read_status(dev) == 6
+    (l0, lp, dO, dP), (l1, lp1, dO1, dP1) = [[x.cpu().numpy() for x in r] for r in runs]
+    assert np.array_equal(lp, lp1, equal_nan=True) and np.array_equal(dO, dO1) and np.array_equal(dP, dP1)
+    skipped = ids == ids[140]
+    assert np.all(np.isnan(lp[skipped])) and np.all(np.isfinite(lp[~skipped]))
+    keep = ids[~skipped]
+    r = fm.fwd_adj(O, P, tlY[keep], tlX[keep], Imeas[keep], "Poisson_likelihood_loss")
+    assert np.all(np.abs(lp[~skipped] - r["loss"]) <= 2e-5 * np.abs(r["loss"]))
+    assert rel_max(dO, r["dO"]) <= 2e-4, rel_max(dO, r["dO"])
+    assert rel_max(dP, r["dP"]) <= 2e-4, rel_max(dP, r["dP"])
+    assert pkg.read_status(dev) == 0
+
+
+def test_intensity_gradient_256(pkg):
+    """The intensity-gradient call (autograd of forward_intensity_batched)
+    over two chunks, against the FP64 adjoint."""
+    dev = torch.device("cuda")
+    B = 70
+    O, P, tlY, tlX, _ = _case(M, 400, B, seed=31)
+    gI = np.random.default_rng(4).standard_normal((B, M, M)).astype(np.float32)
+    Ot = torch.from_numpy(O).to(dev).requires_grad_(True)
+    Pt = torch.from_numpy(P).to(dev).requires_grad_(True)
+    I = pkg.forward_intensity_batched(Ot, Pt, pkg.make_windows(tlY, tlX, dev))
+    (I * torch.from_numpy(gI).to(dev)).sum().backward()
+    dO, dP = _intensity_grad_ref(O, P, tlY, tlX, gI.astype(np.float64))
+    assert rel_max(Ot.grad.cpu().numpy(), dO) <= 2e-4, rel_max(Ot.grad.cpu().numpy(), dO)
+    assert rel_max(Pt.grad.cpu().numpy(), dP) <= 2e-4, rel_max(Pt.grad.cpu().numpy(), dP)
