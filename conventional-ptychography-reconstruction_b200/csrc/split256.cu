@@ -12,9 +12,8 @@
 //   C  rows:     E'_b[y][.] = IDFT_x(X_b[y][.]); per-pattern loss from the
 //                column-block partials in a fixed order
 // so E'_b = (-1)^(x+y) dL/dpsi_b, the layout the assembly (assemble.cu)
-// reads.  X_b is E'_b's own workspace slot: no other scratch.  Patterns run
-// in chunks of kChunk so a chunk's slots stay in L2 between the three
-// kernels.
+// reads.  X_b is E'_b's own workspace slot: no other scratch.  Batches
+// above kChunk patterns run in chunks of kChunk.
 //
 // Line DFT of length 256 = 16 x 16.  Rows: a half-warp per row, lane j
 // holding x[j + 16 k] in registers; a 16-point DFT over k, the twiddle
@@ -32,11 +31,18 @@
 #include "dft_regs.cuh"
 #include "fused.cuh"
 
+// Build-time tuning (measured on B200, c3 = 64 and c4 = 512 patterns): one
+// launch per kernel for up to 512 patterns beat chunks of 64 that keep the
+// scratch in L2 (c4 515 vs 551 us: fuller waves, fewer launches); three
+// column CTAs per SM at 85 registers beat four at 64 with a 20-byte spill.
 #ifndef PTY_S256_CHUNK
-#define PTY_S256_CHUNK 64
+#define PTY_S256_CHUNK 512
 #endif
 #ifndef PTY_S256_COLS_MINB
-#define PTY_S256_COLS_MINB 4
+#define PTY_S256_COLS_MINB 3
+#endif
+#ifndef PTY_S256_ROWS_MINB
+#define PTY_S256_ROWS_MINB 4
 #endif
 
 namespace pty {
@@ -108,7 +114,7 @@ PTY_DEVI bool window_ok(const FusedArgs& a, int b, int& f, int2& w) {
 // A: gather + row DFTs.  grid (NCB, chunk): CTA (rb, b - b0) owns rows
 // 16 rb .. 16 rb + 15 of pattern b.  Also resolves the window (tlb, status)
 // and, once per call, zeroes the assembly's dP arrival counters.
-__global__ void __launch_bounds__(NT, 4) k_rows_fwd(const Args g) {
+__global__ void __launch_bounds__(NT, PTY_S256_ROWS_MINB) k_rows_fwd(const Args g) {
   extern __shared__ __align__(16) unsigned char smem[];
   float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
   float* pre = reinterpret_cast<float*>(smem + SM_RE);
@@ -151,7 +157,7 @@ __global__ void __launch_bounds__(NT, 4) k_rows_fwd(const Args g) {
 // C: inverse row DFTs in place -> E'.  grid (NCB, chunk).  CTA (0, b)
 // also writes the pattern's loss: its NCB column-block partials summed in
 // order, / M^2 (NaN for a skipped window).
-__global__ void __launch_bounds__(NT, 4) k_rows_inv(const Args g) {
+__global__ void __launch_bounds__(NT, PTY_S256_ROWS_MINB) k_rows_inv(const Args g) {
   extern __shared__ __align__(16) unsigned char smem[];
   float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
   float* pre = reinterpret_cast<float*>(smem + SM_RE);

@@ -1,6 +1,6 @@
 """Parity of the 256 x 256 probe paths with the FP64 oracle: the line-DFT
-kernels (smooth-L1, Poisson and the intensity gradient; patterns in chunks of
-64) and the 4-CTA cluster kernel (FD loss and forward intensities; the
+kernels (smooth-L1, Poisson and the intensity gradient; batches above 512
+patterns in chunks of 512) and the 4-CTA cluster kernel (FD loss and forward intensities; the
 pass-2/pass-3 exchange through distributed shared memory).
 
 Tolerances as for 64 / 128 (FP32 FFT against FP64):
@@ -117,16 +117,29 @@ def _intensity_grad_ref(O, P, tlY, tlX, gI):
     return dO, dP
 
 
+def _oracle_chunked(O, P, tlY, tlX, Imeas, loss_type, chunk=64):
+    loss = np.empty(tlY.size)
+    dO = np.zeros(O.shape, np.complex128)
+    dP = np.zeros(P.shape, np.complex128)
+    for s in range(0, tlY.size, chunk):
+        r = fm.fwd_adj(O, P, tlY[s:s + chunk], tlX[s:s + chunk], Imeas[s:s + chunk], loss_type)
+        loss[s:s + chunk] = r["loss"]
+        dO += r["dO"]
+        dP += r["dP"]
+    return loss, dO, dP
+
+
 def test_chunks_repeats_and_a_skipped_window_256(pkg):
-    """150 patterns = chunks of 64, 64 and 22; frame ids repeat; one window in
-    the last chunk leaves the canvas (NaN loss, status 6, no contribution);
-    bitwise repeatable."""
+    """520 patterns = the line-DFT kernels' chunks of 512 and 8; frame ids
+    repeat; one frame's window, drawn in the second chunk, leaves the canvas
+    (NaN loss wherever it is drawn, status 6, no contribution); bitwise
+    repeatable."""
     dev = torch.device("cuda")
-    H, F = 460, 40
+    H, F, B = 460, 40, 520
     O, P, tlY, tlX, Imeas = _case(M, H, F, seed=150)
-    ids = np.random.default_rng(3).integers(0, F, 150).astype(np.int32)
+    ids = np.random.default_rng(3).integers(0, F, B).astype(np.int32)
     bad = tlX.copy()
-    bad[ids[140]] = H - M + 3
+    bad[ids[515]] = H - M + 3
     Ot, Pt = torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev)
     tl = pkg.make_windows(tlY, bad, dev)
     Im = torch.from_numpy(Imeas).to(dev)
@@ -138,13 +151,14 @@ def test_chunks_repeats_and_a_skipped_window_256(pkg):
     assert pkg.read_status(dev) == 6
     (l0, lp, dO, dP), (l1, lp1, dO1, dP1) = [[x.cpu().numpy() for x in r] for r in runs]
     assert np.array_equal(lp, lp1, equal_nan=True) and np.array_equal(dO, dO1) and np.array_equal(dP, dP1)
-    skipped = ids == ids[140]
+    skipped = ids == ids[515]
     assert np.all(np.isnan(lp[skipped])) and np.all(np.isfinite(lp[~skipped]))
     keep = ids[~skipped]
-    r = fm.fwd_adj(O, P, tlY[keep], tlX[keep], Imeas[keep], "Poisson_likelihood_loss")
-    assert np.all(np.abs(lp[~skipped] - r["loss"]) <= 2e-5 * np.abs(r["loss"]))
-    assert rel_max(dO, r["dO"]) <= 2e-4, rel_max(dO, r["dO"])
-    assert rel_max(dP, r["dP"]) <= 2e-4, rel_max(dP, r["dP"])
+    ref_l, ref_dO, ref_dP = _oracle_chunked(O.astype(np.complex128), P.astype(np.complex128), tlY[keep], tlX[keep],
+                                            Imeas[keep], "Poisson_likelihood_loss")
+    assert np.all(np.abs(lp[~skipped] - ref_l) <= 2e-5 * np.abs(ref_l))
+    assert rel_max(dO, ref_dO) <= 2e-4, rel_max(dO, ref_dO)
+    assert rel_max(dP, ref_dP) <= 2e-4, rel_max(dP, ref_dP)
     assert pkg.read_status(dev) == 0
 
 
