@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "assemble.cuh"
 #include "fused.cuh"
 #include "general.cuh"
@@ -24,8 +26,9 @@ static WsLayout ws_layout(int M, int N, int B) {
   off += pty_align_up(size_t(B) * MN * sizeof(float2), 256);
   L.scr = off;  // the general path's FD planes
   if (!fused_probe(M, N)) off += pty_align_up(size_t(B) * MN * 3 * sizeof(float), 256);
-  L.part = off;
-  off += pty_align_up(G * MN * sizeof(float2), 256);
+  L.part = off;  // dP group partials: the assembly's groups of kGroup, or the M = 256 path's of kDpGroup
+  const size_t GP = (M == 256 && N == 256) ? std::max(G, (size_t(B) + kDpGroup - 1) / kDpGroup) : G;
+  off += pty_align_up(GP * MN * sizeof(float2), 256);
   L.loss = off;
   off += pty_align_up(size_t(B) * sizeof(double), 256);
   L.tlb = off;
@@ -175,14 +178,23 @@ int ptycho_fwd_adj(const float* O, int H, int W, const float* P, int M, int N, c
   const bool fused = fused_probe(M, N);
   const int mode = adj ? MODE_ADJ : MODE_LOSS;
   if (fused && M == 256 && split256_supported(mode, loss_type)) {
-    // the line-DFT kernels use E' as their scratch in both modes
+    // the line-DFT kernels use E' as their scratch in both modes; on large
+    // batches the probe gradient comes out of the inverse-row kernel
     a.Eout = Ews;
     a.tlb = tlb;
     if (adj) {
       a.done = done;
       a.ndone = dp_counters(M, N);
     }
-    st = launch_split256(mode, loss_type, a, reinterpret_cast<double*>(ws + L.lpart), s);
+    const bool dp_fused = adj && dP && B >= kDpFuseMinB;
+    st = launch_split256(mode, loss_type, a, reinterpret_cast<double*>(ws + L.lpart), dp_fused ? part : nullptr, s);
+    if (st) return st;
+    if (dp_fused) {
+      st = launch_assemble(Ews, reinterpret_cast<const float2*>(O), reinterpret_cast<const float2*>(P), tlb, B, H,
+                           W, M, N, true, reinterpret_cast<float2*>(dO), nullptr, part, done, lp, nullptr, acc, s);
+      if (st) return st;
+      return split256_dp_sum(part, B, reinterpret_cast<float2*>(dP), acc, lp, loss_total, s);
+    }
   } else if (fused) {
     if (adj) {
       a.Eout = Ews;

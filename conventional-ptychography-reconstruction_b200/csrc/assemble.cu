@@ -25,31 +25,8 @@
 
 namespace pty {
 
-PTY_DEVI float2 c_negif(float2 a, int odd) { return odd ? make_float2(-a.x, -a.y) : a; }
-
-// acc += a * conj(b), as two FMAs per component
-PTY_DEVI void c_fma_conj(float2& acc, float2 a, float2 b) {
-  acc.x = fmaf(a.x, b.x, fmaf(a.y, b.y, acc.x));
-  acc.y = fmaf(a.y, b.x, fmaf(-a.x, b.y, acc.y));
-}
-
 PTY_DEVI float2 c_xor_sign(float2 a, unsigned m) {
   return make_float2(__uint_as_float(__float_as_uint(a.x) ^ m), __uint_as_float(__float_as_uint(a.y) ^ m));
-}
-
-PTY_DEVI void loss_sum_block(const double* __restrict__ loss_pat, int B, double* loss_total) {
-  __shared__ double red[8];
-  double s = 0.0;
-  for (int b = threadIdx.x; b < B; b += 256) s += loss_pat[b];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int i = 0; i < 8; ++i) t += red[i];
-    loss_total[0] = t;
-  }
 }
 
 __global__ void __launch_bounds__(256) k_loss_total(const double* __restrict__ loss_pat, int B,

@@ -12,6 +12,24 @@ constexpr int kPixBlock = 256;  // probe pixels per dP block
 // before the first call; every call leaves them zeroed)
 inline int dp_counters(int M, int N) { return (M * N + kPixBlock - 1) / kPixBlock; }
 
+// FP64 sum of the per-pattern losses in a fixed order (a strided pass per
+// thread, a shuffle tree, the eight warp sums in order) by one block of 256
+// threads; every thread of the block calls it
+PTY_DEVI void loss_sum_block(const double* __restrict__ loss_pat, int B, double* loss_total) {
+  __shared__ double red[8];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < B; b += 256) s += loss_pat[b];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < 8; ++i) t += red[i];
+    loss_total[0] = t;
+  }
+}
+
 // dP (group partials, then the last-arriving block sums them in group order),
 // dO (tile owner sums in ascending pattern order) and the FP64 loss total in
 // one launch; any output may be null.  E' is only read; with fftshift_sign

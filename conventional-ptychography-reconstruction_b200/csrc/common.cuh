@@ -20,6 +20,12 @@ PTY_DEVI float2 c_mulc(float2 a, float2 b) {
 }
 PTY_DEVI float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
 PTY_DEVI float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+PTY_DEVI float2 c_negif(float2 a, int odd) { return odd ? make_float2(-a.x, -a.y) : a; }
+// acc += a * conj(b), as two FMAs per component
+PTY_DEVI void c_fma_conj(float2& acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, fmaf(a.y, b.y, acc.x));
+  acc.y = fmaf(a.y, b.x, fmaf(-a.x, b.y, acc.y));
+}
 
 // Record an error code in a device status word (first writer wins; never cleared).
 PTY_DEVI void pty_raise(int32_t* status, int code) {

@@ -370,9 +370,20 @@ int launch_fused_256(int mode, int loss, const FusedArgs& a, cudaStream_t s);
 
 // split256.cu: M = 256 as three line-DFT kernels (smooth-L1, Poisson and the
 // intensity-gradient losses in MODE_LOSS / MODE_ADJ); a.Eout is the scratch,
-// lpart holds B * kSplit256Blocks doubles
+// lpart holds B * kSplit256Blocks doubles.  With dp_part (MODE_ADJ, batches of
+// at least kDpFuseMinB patterns) the inverse-row kernel also leaves the probe
+// gradient as ceil(B / kDpGroup) partials of 256 x 256 in dp_part, which
+// split256_dp_sum adds into dP (and writes the loss total); the assembly then
+// runs without its dP role.
 constexpr int kSplit256Blocks = 16;
+constexpr int kDpGroup = 8;
+#ifndef PTY_S256_DP_FUSE_MIN_B
+#define PTY_S256_DP_FUSE_MIN_B 192
+#endif
+constexpr int kDpFuseMinB = PTY_S256_DP_FUSE_MIN_B;
 bool split256_supported(int mode, int loss);
-int launch_split256(int mode, int loss, const FusedArgs& a, double* lpart, cudaStream_t s);
+int launch_split256(int mode, int loss, const FusedArgs& a, double* lpart, float2* dp_part, cudaStream_t s);
+int split256_dp_sum(const float2* dp_part, int B, float2* dP, bool accumulate, const double* loss_pat,
+                    double* loss_total, cudaStream_t s);
 
 }  // namespace pty

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "assemble.cuh"
 #include "dft_regs.cuh"
 #include "fused.cuh"
 
@@ -56,6 +57,7 @@ constexpr int BUF = LINES * 16 * TP;  // floats per plane (re or im): 4352
 constexpr int NCB = M / LINES;     // column (or row) blocks per pattern: 16
 static_assert(NCB == kSplit256Blocks, "loss partials per pattern");
 constexpr int kChunk = PTY_S256_CHUNK;
+static_assert(kChunk % kDpGroup == 0, "probe-gradient groups do not straddle chunks");
 
 // shared memory: twiddles, two transpose planes (re, im), reduction
 constexpr size_t SM_TW = 0;
@@ -71,10 +73,14 @@ struct Args {
   int b0;         // first pattern of this chunk
 };
 
-// W256^k, k = 0..255 (forward sign), one entry per thread
+// The line twiddles W256^(j p), j, p = 0..15 (forward sign), stored at
+// p * 16 + j: the row lanes j of a half-warp read 16 adjacent entries (no bank
+// conflict), the column half-warps read one entry (a broadcast).  One entry
+// per thread.
 PTY_DEVI void fill_twiddles(float2* tw) {
+  const int p = threadIdx.x >> 4, j = threadIdx.x & 15;
   float s, c;
-  sincospif(-float(threadIdx.x) / 128.0f, &s, &c);
+  sincospif(-float(j * p) / 128.0f, &s, &c);
   tw[threadIdx.x] = make_float2(c, s);
 }
 
@@ -86,7 +92,7 @@ PTY_DEVI void line256(float2 (&v)[16], int j, float* bre, float* bim, const floa
   dft16<INV, 1>(v);  // v[p] = sum_k x[j + 16 k] W16^(k p)
 #pragma unroll
   for (int p = 1; p < 16; ++p) {
-    const float2 w = tw[(j * p) & (M - 1)];
+    const float2 w = tw[p * 16 + j];
     v[p] = c_mul(v[p], INV ? c_conj(w) : w);
   }
   __syncwarp();
@@ -184,6 +190,102 @@ __global__ void __launch_bounds__(NT, PTY_S256_ROWS_MINB) k_rows_inv(const Args 
   for (int q = 0; q < 16; ++q) Xr[16 * q] = v[q];
 }
 
+// C with the probe gradient (large batches): grid (NCB, groups of kDpGroup
+// patterns).  The CTA runs C for rows 16 rb .. 16 rb + 15 of its group's
+// patterns in ascending order and, while E' is in registers, accumulates
+// sum_b E'_b conj(O_b) over those rows; the group's partial, with the
+// (-1)^(x+y) factor applied once, goes to part[group].  The assembly then
+// never reads E' for dP (it reads it once, for dO), and k_dp_sum adds the
+// partials in group order.
+__global__ void __launch_bounds__(NT, 2) k_rows_inv_dp(const Args g, float2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* tw = reinterpret_cast<float2*>(smem + SM_TW);
+  float* pre = reinterpret_cast<float*>(smem + SM_RE);
+  float* pim = reinterpret_cast<float*>(smem + SM_IM);
+  const FusedArgs& a = g.f;
+  const int t = threadIdx.x, r = t >> 4, j = t & 15;
+  const int y = blockIdx.x * LINES + r;
+  const int grp = g.b0 / kDpGroup + blockIdx.y;
+  const int b1 = min(a.B, (grp + 1) * kDpGroup);
+  fill_twiddles(tw);
+  __syncthreads();
+  float2 acc[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) acc[q] = make_float2(0.f, 0.f);
+  for (int b = grp * kDpGroup; b < b1; ++b) {
+    const int2 w = __ldg(a.tlb + b);
+    const bool ok = w.x >= 0;
+    if (blockIdx.x == 0 && t == 0 && a.loss_pat) {
+      double s = 0.0;
+      for (int cb = 0; cb < NCB; ++cb) s += g.lpart[size_t(b) * NCB + cb];
+      a.loss_pat[b] = ok ? s / double(M * M) : (double)__int_as_float(0x7fc00000);
+    }
+    if (!ok) continue;  // uniform over the CTA
+    float2* Xr = a.Eout + size_t(b) * M * M + size_t(y) * M + j;
+    float2 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = Xr[16 * k];
+    line256<true>(v, j, pre + r * 16 * TP, pim + r * 16 * TP, tw);
+    const float2* Or = a.O + size_t(w.x + y) * a.W + w.y + j;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      Xr[16 * q] = v[q];
+      c_fma_conj(acc[q], v[q], __ldg(Or + 16 * q));
+    }
+  }
+  float2* pr = part + size_t(grp) * M * M + size_t(y) * M + j;
+  const int odd = (j + y) & 1;  // x = j + 16 q has the parity of j
+#pragma unroll
+  for (int q = 0; q < 16; ++q) __stcg(pr + 16 * q, c_negif(acc[q], odd));
+}
+
+// dP = (accumulate ? dP : 0) + sum over groups of part[group], in group
+// order: four threads per pixel pair each add a quarter of the groups (eight
+// loads in flight), then the quarters are added in order.  Block 0 also
+// writes the FP64 loss total.
+__global__ void __launch_bounds__(256) k_dp_sum(const float2* __restrict__ part, int ngroups,
+                                                 float2* __restrict__ dP, int accumulate,
+                                                 const double* __restrict__ loss_pat, int B, double* loss_total) {
+  __shared__ float4 quarter[4][64];
+  const int qd = threadIdx.x >> 6, pl = threadIdx.x & 63;
+  const int i = blockIdx.x * 64 + pl;  // pixel pair
+  const float4* p4 = reinterpret_cast<const float4*>(part) + i;
+  constexpr size_t kStride = M * M / 2;
+  const int gq = (ngroups + 3) / 4;
+  const int g1 = min(ngroups, (qd + 1) * gq);
+  float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+  int gi = qd * gq;
+  for (; gi + 8 <= g1; gi += 8) {
+    float4 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = __ldcg(p4 + size_t(gi + u) * kStride);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s = make_float4(s.x + v[u].x, s.y + v[u].y, s.z + v[u].z, s.w + v[u].w);
+  }
+  for (; gi < g1; ++gi) {
+    const float4 v = __ldcg(p4 + size_t(gi) * kStride);
+    s = make_float4(s.x + v.x, s.y + v.y, s.z + v.z, s.w + v.w);
+  }
+  quarter[qd][pl] = s;
+  __syncthreads();
+  if (qd == 0) {
+    s = quarter[0][pl];
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+      const float4 v = quarter[k][pl];
+      s = make_float4(s.x + v.x, s.y + v.y, s.z + v.z, s.w + v.w);
+    }
+    float2* d = dP + 2 * i;  // dP is only required to be 8-byte aligned
+    if (accumulate) {
+      const float2 o0 = d[0], o1 = d[1];
+      s = make_float4(o0.x + s.x, o0.y + s.y, o1.x + s.z, o1.y + s.w);
+    }
+    d[0] = make_float2(s.x, s.y);
+    d[1] = make_float2(s.z, s.w);
+  }
+  if (blockIdx.x == 0 && loss_total) loss_sum_block(loss_pat, B, loss_total);
+}
+
 // 256-point DFT of one column per thread slot, spread over the CTA: thread
 // (j, c) = (t >> 4, t & 15) holds x[j + 16 k] of column c in v[k]; a 16-point
 // DFT over k, the twiddle W256^(j p), a transpose across warps through the
@@ -198,7 +300,7 @@ PTY_DEVI void col256(float2 (&v)[16], int j, int c, float* bre, float* bim, cons
   dft16<INV, 1>(v);
 #pragma unroll
   for (int p = 1; p < 16; ++p) {
-    const float2 w = tw[(j * p) & (M - 1)];
+    const float2 w = tw[p * 16 + j];
     v[p] = c_mul(v[p], INV ? c_conj(w) : w);
   }
   __syncthreads();  // earlier readers of the planes are done
@@ -301,15 +403,15 @@ static bool set_smem(K kern, size_t bytes, PtyDevCache& cache) {
 }
 
 template <int LOSS>
-static int launch_t(bool adj, const FusedArgs& fa, double* lpart, cudaStream_t s) {
+static int launch_t(bool adj, const FusedArgs& fa, double* lpart, float2* dp_part, cudaStream_t s) {
   // "shared-memory attribute set" per device and kernel; cleared when a
   // launch is refused (a device reset drops the attribute), so the next
   // call sets it again
-  static PtyDevCache c_rows_fwd, c_rows_inv, c_cols_adj, c_cols_loss;
+  static PtyDevCache c_rows_fwd, c_rows_inv, c_rows_inv_dp, c_cols_adj, c_cols_loss;
   PtyDevCache& c_cols = adj ? c_cols_adj : c_cols_loss;
   auto kcols = adj ? k_cols<LOSS, true> : k_cols<LOSS, false>;
   if (!set_smem(k_rows_fwd, SMEM_ROWS, c_rows_fwd) || !set_smem(k_rows_inv, SMEM_ROWS, c_rows_inv) ||
-      !set_smem(kcols, SMEM_COLS, c_cols))
+      !set_smem(k_rows_inv_dp, SMEM_ROWS, c_rows_inv_dp) || !set_smem(kcols, SMEM_COLS, c_cols))
     return PTYCHO_ERR_LAUNCH;
   Args g{fa, lpart, 0};
   for (int b0 = 0; b0 < fa.B; b0 += kChunk) {
@@ -318,12 +420,15 @@ static int launch_t(bool adj, const FusedArgs& fa, double* lpart, cudaStream_t s
     const dim3 grid(NCB, n);
     k_rows_fwd<<<grid, NT, SMEM_ROWS, s>>>(g);
     kcols<<<grid, NT, SMEM_COLS, s>>>(g);
-    if (adj) k_rows_inv<<<grid, NT, SMEM_ROWS, s>>>(g);
+    if (adj && dp_part)
+      k_rows_inv_dp<<<dim3(NCB, (n + kDpGroup - 1) / kDpGroup), NT, SMEM_ROWS, s>>>(g, dp_part);
+    else if (adj)
+      k_rows_inv<<<grid, NT, SMEM_ROWS, s>>>(g);
   }
   if (!adj) k_loss_pat<<<(fa.B + 255) / 256, 256, 0, s>>>(g);
   if (cudaGetLastError() == cudaSuccess) return PTYCHO_OK;
   int dev;
-  for (PtyDevCache* c : {&c_rows_fwd, &c_rows_inv, &c_cols})
+  for (PtyDevCache* c : {&c_rows_fwd, &c_rows_inv, &c_rows_inv_dp, &c_cols})
     if (c->get(&dev)) c->put(dev, 0);
   return PTYCHO_ERR_LAUNCH;
 }
@@ -340,15 +445,23 @@ bool split256_supported(int mode, int loss) {
 
 // a.Eout (B M^2 complex64) is the scratch and, in MODE_ADJ, the output E';
 // a.tlb receives the resolved windows in both modes; lpart holds B * 16 doubles
-int launch_split256(int mode, int loss, const FusedArgs& a, double* lpart, cudaStream_t s) {
+int launch_split256(int mode, int loss, const FusedArgs& a, double* lpart, float2* dp_part, cudaStream_t s) {
   using namespace s256;
   if (!split256_supported(mode, loss) || !a.Eout || !a.tlb || !lpart) return PTYCHO_ERR_INVALID_ARG;
   const bool adj = mode == MODE_ADJ;
   switch (loss) {
-    case PTYCHO_LOSS_SMOOTH_L1: return launch_t<PTYCHO_LOSS_SMOOTH_L1>(adj, a, lpart, s);
-    case PTYCHO_LOSS_POISSON: return launch_t<PTYCHO_LOSS_POISSON>(adj, a, lpart, s);
-    default: return launch_t<PTYCHO_LOSS_INTENSITY_GRAD>(adj, a, lpart, s);
+    case PTYCHO_LOSS_SMOOTH_L1: return launch_t<PTYCHO_LOSS_SMOOTH_L1>(adj, a, lpart, dp_part, s);
+    case PTYCHO_LOSS_POISSON: return launch_t<PTYCHO_LOSS_POISSON>(adj, a, lpart, dp_part, s);
+    default: return launch_t<PTYCHO_LOSS_INTENSITY_GRAD>(adj, a, lpart, dp_part, s);
   }
+}
+
+int split256_dp_sum(const float2* dp_part, int B, float2* dP, bool accumulate, const double* loss_pat,
+                    double* loss_total, cudaStream_t s) {
+  using namespace s256;
+  const int ngroups = (B + kDpGroup - 1) / kDpGroup;
+  k_dp_sum<<<M * M / 2 / 64, 256, 0, s>>>(dp_part, ngroups, dP, accumulate ? 1 : 0, loss_pat, B, loss_total);
+  return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 
 }  // namespace pty

@@ -160,6 +160,15 @@ def test_chunks_repeats_and_a_skipped_window_256(pkg):
     assert rel_max(dO, ref_dO) <= 2e-4, rel_max(dO, ref_dO)
     assert rel_max(dP, ref_dP) <= 2e-4, rel_max(dP, ref_dP)
     assert pkg.read_status(dev) == 0
+    # accumulate: two calls into the same buffers give twice one call (this
+    # batch size takes the probe gradient from the inverse-row kernel)
+    gO = torch.zeros_like(Ot)
+    gP = torch.zeros_like(Pt)
+    for _ in range(2):
+        pkg.fwd_adj_raw(Ot, Pt, tl, Im, pkg.LOSS_CODES["Poisson_likelihood_loss"], batch=bt, dO=gO, dP=gP,
+                        accumulate=True)
+    pkg.read_status(dev, reset=True)
+    assert rel_max(gO.cpu().numpy(), 2 * dO) <= 1e-6 and rel_max(gP.cpu().numpy(), 2 * dP) <= 1e-6
 
 
 def test_intensity_gradient_256(pkg):
