@@ -22,14 +22,16 @@
 // 16-value register slots; lines up to 1024 points use 8 for more threads) --
 // natural order in and out, each thread holding one or two slots in
 // registers, in place between barriers -- remaps the spectrum, runs the
-// inverse passes and writes the lines back.  Twiddles come from a per-CTA
-// table exp(-2 pi i k / LMAX) rounded from double-precision sincospi.
+// inverse passes and writes the lines back.  Twiddles come from the
+// correctly rounded build-time table kTw4096 (twiddle4096.cuh, read through
+// the L1 cache with stride 4096 / L), so no CTA spends time building one.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "common.cuh"
 #include "dft_regs.cuh"
 #include "line_fft.cuh"
+#include "twiddle4096.cuh"
 
 namespace pty {
 namespace rs {
@@ -41,7 +43,8 @@ template <int L1, int L2, bool COL>
 struct Cfg {
   static constexpr int LMAX = cmax(L1, L2);
   // row pass: 2048 values per CTA (>= 1 line); column pass: >= 4 lines
-  // (32-byte segments) and 4096 values per CTA when lines are short
+  // (32-byte segments) and 4096 values per CTA when lines are short (2 lines
+  // of 4096, which would fit three CTAs per SM, ran slower: 16-byte pieces)
   static constexpr int LINES = COL ? cmax(4, 4096 / LMAX) : cmax(1, 2048 / LMAX);
   static constexpr int N = LINES * LMAX;            // values held by the CTA
   // values per register slot: 8 (radix-8 passes) for lines up to 1024 points,
@@ -50,7 +53,7 @@ struct Cfg {
   static constexpr int NT = cmin(512, N / VPT);     // threads: one slot each, or two
   static constexpr int SPT = N / VPT / NT;          // slots per thread (1 or 2)
   static constexpr int PLANE = N + N / 32;          // padded plane length (floats)
-  static constexpr size_t SMEM = size_t(2) * PLANE * 4 + size_t(LMAX) * 8;
+  static constexpr size_t SMEM = size_t(2) * PLANE * 4;
   static_assert(SPT == 1 || SPT == 2, "slot count");
   static_assert(L1 >= 64 && L2 >= 64 && LMAX <= 4096, "supported line lengths");
 };
@@ -59,14 +62,15 @@ PTY_DEVI int pad(int i) { return i + (i >> 5); }
 
 // One Stockham pass of radix R over every line of length L: butterfly j of a
 // line reads j + r L/R, applies exp(-+2 pi i (j mod NS) r / (NS R)) and the
-// radix-R DFT, and writes (j / NS) NS R + (j mod NS) + r NS.
+// radix-R DFT, and writes (j / NS) NS R + (j mod NS) + r NS.  Twiddles are
+// read from the 4096-entry table kTw4096 (global memory, L1-cached).
 template <int L, int R, int NS, bool INV, int LINES, int NT, int SPT, int LMAX, int VPT>
-PTY_DEVI void stockham(float* re, float* im, const float2* __restrict__ tw, int t) {
+PTY_DEVI void stockham(float* re, float* im, int t) {
   constexpr int BPL = L / R;              // butterflies per line
   constexpr int NB = LINES * BPL;         // butterflies in the CTA
   constexpr int PER = VPT / R;            // butterflies per VPT-value slot
   constexpr int NSLOT = NB / PER;         // slots in use (<= SPT * NT)
-  constexpr int TWS = LMAX / (NS * R);    // twiddle table stride
+  constexpr int TWS = 4096 / (NS * R);    // twiddle table stride
   float2 v[SPT][VPT];
   int jj[SPT][PER], base[SPT][PER];
 #pragma unroll
@@ -99,7 +103,7 @@ PTY_DEVI void stockham(float* re, float* im, const float2* __restrict__ tw, int 
         if constexpr (NS > 1) {
 #pragma unroll
           for (int r = 1; r < R; ++r) {
-            float2 w = tw[k * r * TWS];
+            float2 w = __ldg(&kTw4096[k * r * TWS]);
             if constexpr (INV) w.y = -w.y;
             v[q][p * R + r] = c_mul(v[q][p * R + r], w);
           }
@@ -120,12 +124,12 @@ PTY_DEVI void stockham(float* re, float* im, const float2* __restrict__ tw, int 
 
 // all passes of a length-L transform: radix VPT while it divides the rest, then smaller
 template <int L, bool INV, int LINES, int NT, int SPT, int LMAX, int VPT, int NS = 1>
-PTY_DEVI void fft_lines(float* re, float* im, const float2* tw, int t) {
+PTY_DEVI void fft_lines(float* re, float* im, int t) {
   if constexpr (NS < L) {
     constexpr int REST = L / NS;
     constexpr int R = REST >= VPT ? VPT : REST;
-    stockham<L, R, NS, INV, LINES, NT, SPT, LMAX, VPT>(re, im, tw, t);
-    fft_lines<L, INV, LINES, NT, SPT, LMAX, VPT, NS * R>(re, im, tw, t);
+    stockham<L, R, NS, INV, LINES, NT, SPT, LMAX, VPT>(re, im, t);
+    fft_lines<L, INV, LINES, NT, SPT, LMAX, VPT, NS * R>(re, im, t);
   }
 }
 
@@ -139,14 +143,8 @@ __global__ void __launch_bounds__(Cfg<L1, L2, COL>::NT) k_resample(const float2*
   extern __shared__ __align__(16) unsigned char smem[];
   float* re = reinterpret_cast<float*>(smem);
   float* im = re + C::PLANE;
-  float2* tw = reinterpret_cast<float2*>(im + C::PLANE);
   const int t = threadIdx.x;
   const int l0 = blockIdx.x * LINES;
-  for (int k = t; k < LMAX; k += NT) {
-    double s, c;
-    sincospi(-2.0 * double(k) / double(LMAX), &s, &c);
-    tw[k] = make_float2(float(c), float(s));
-  }
   // load LINES lines of length L1 (lines past the end read as zero)
   for (int idx = t; idx < LINES * L1; idx += NT) {
     int l, k;
@@ -165,7 +163,7 @@ __global__ void __launch_bounds__(Cfg<L1, L2, COL>::NT) k_resample(const float2*
     im[i] = x.y;
   }
   __syncthreads();
-  fft_lines<L1, false, LINES, NT, C::SPT, LMAX, C::VPT>(re, im, tw, t);
+  fft_lines<L1, false, LINES, NT, C::SPT, LMAX, C::VPT>(re, im, t);
   // spectrum remap: frequency f in [-n/2, n/2), n = min(L1, L2), from f mod L1 to f mod L2
   if constexpr (L2 > L1) {
     for (int idx = t; idx < LINES * (L1 / 2); idx += NT) {  // negative frequencies move up
@@ -191,7 +189,7 @@ __global__ void __launch_bounds__(Cfg<L1, L2, COL>::NT) k_resample(const float2*
     }
     __syncthreads();
   }
-  fft_lines<L2, true, LINES, NT, C::SPT, LMAX, C::VPT>(re, im, tw, t);
+  fft_lines<L2, true, LINES, NT, C::SPT, LMAX, C::VPT>(re, im, t);
   for (int idx = t; idx < LINES * L2; idx += NT) {
     int l, k;
     if constexpr (COL) {
