@@ -242,31 +242,64 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) k_cmlp(const Args a) {
   float om1 = 0.f, om2 = 0.f, om3 = 0.f;
   bool first = true;
   const int ntiles = (a.N + 127) / 128;
+  // this half's 16 of row c's 32 input features (and, backward, G_y of row c)
+  auto load_inputs = [&](int cc, float (&xv)[16], float2& g) {
+    const bool ok = cc < a.N;
+    if (a.x_planar) {  // per feature, a warp reads 32 consecutive rows
+#pragma unroll
+      for (int i = 0; i < 16; ++i) xv[i] = ok ? __ldg(a.x + size_t(16 * hh + i) * a.N + cc) : 0.f;
+    } else {
+      const float4* xp = reinterpret_cast<const float4*>(a.x + size_t(ok ? cc : 0) * 32 + 16 * hh);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float4 v = ok ? __ldg(xp + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        xv[4 * q] = v.x;
+        xv[4 * q + 1] = v.y;
+        xv[4 * q + 2] = v.z;
+        xv[4 * q + 3] = v.w;
+      }
+    }
+    if constexpr (BWD) g = (ok && hh == 0) ? __ldg(a.gy + cc) : make_float2(0.f, 0.f);
+  };
+  // The tile loop is a chain of dependent MMA / elementwise steps, so a tile's
+  // input loads would stall it: the backward (registers to spare) loads the
+  // next tile's inputs while this tile computes; the forward (at its register
+  // cap) has them prefetched into L2.
+  auto prefetch_l2 = [&](int nt) {
+    if (nt < ntiles) {
+      if (a.x_planar) {  // 32 features x 512 bytes: one 64-byte piece per thread
+        const int f = t >> 3, piece = t & 7;
+        const int r0 = nt * 128 + piece * 16;
+        if (r0 < a.N) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.x + size_t(f) * a.N + r0));
+      } else {  // 128 rows x 128 bytes: 16 KB, one 64-byte piece per thread
+        const size_t off = size_t(nt) * 128 * 32 + size_t(t) * 16;
+        if (off < size_t(a.N) * 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.x + off));
+      }
+    }
+  };
+  float xnext[16];
+  float2 gnext = make_float2(0.f, 0.f);
+  if constexpr (BWD) load_inputs(blockIdx.x * 128 + row, xnext, gnext);
   for (int tile = blockIdx.x; tile < ntiles && !abort; tile += gridDim.x) {
     const int c = tile * 128 + row;
     const bool valid = c < a.N;
-    // -- inputs: this half's 16 of the row's 32 features ------------------------
+    // -- inputs ------------------------------------------------------------------
     {
       float xv[16];
-      if (a.x_planar) {  // per feature, a warp reads 32 consecutive rows
+      float2 g;
+      if constexpr (BWD) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) xv[i] = valid ? __ldg(a.x + size_t(16 * hh + i) * a.N + c) : 0.f;
+        for (int i = 0; i < 16; ++i) xv[i] = xnext[i];
+        g = gnext;
+        load_inputs((tile + gridDim.x) * 128 + row, xnext, gnext);  // lands during this tile
       } else {
-        const float4* xp = reinterpret_cast<const float4*>(a.x + size_t(valid ? c : 0) * 32 + 16 * hh);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const float4 v = valid ? __ldg(xp + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-          xv[4 * q] = v.x;
-          xv[4 * q + 1] = v.y;
-          xv[4 * q + 2] = v.z;
-          xv[4 * q + 3] = v.w;
-        }
+        load_inputs(c, xv, g);
+        prefetch_l2(tile + gridDim.x);
       }
       st8(sm + S_X, row, 16 * hh, xv);
       st8(sm + S_X, row, 16 * hh + 8, xv + 8);
       if constexpr (BWD) {
         if (hh == 0) {
-          const float2 g = valid ? __ldg(a.gy + c) : make_float2(0.f, 0.f);
           const float v8[8] = {g.x, g.y, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
           st8(sm + S_GY, row, 0, v8);
         }
