@@ -130,6 +130,32 @@ __global__ void __launch_bounds__(256) k_hash_fwd_planar(const float2* __restric
   feat[size_t(2 * l + 1) * N + n] = fmaf(w11, t11.y, fmaf(w01, t01.y, fmaf(w10, t10.y, w00 * t00.y)));
 }
 
+// feature-major forward, one thread per coordinate over all levels: the
+// coordinate is read once (not once per level) and each level's two stores
+// are still coalesced across the warp
+__global__ void __launch_bounds__(256) k_hash_fwd_planar_all(const float2* __restrict__ coords, int N,
+                                                             const float2* __restrict__ table, const LevelTable L,
+                                                             float* __restrict__ feat) {
+  const int n = blockIdx.x * 256 + threadIdx.x;
+  if (n >= N) return;
+  const float2 x = __ldg(coords + n);
+#pragma unroll 4
+  for (int l = 0; l < L.levels; ++l) {
+    const float s = L.scale[l];
+    const float px = fmaf(x.x, s, 0.5f), py = fmaf(x.y, s, 0.5f);
+    const float gx = floorf(px), gy = floorf(py);
+    const float fx = px - gx, fy = py - gy;
+    const int ix = int(gx), iy = int(gy);
+    const float2 t00 = __ldg(table + corner_entry(L, l, ix, iy));
+    const float2 t10 = __ldg(table + corner_entry(L, l, ix + 1, iy));
+    const float2 t01 = __ldg(table + corner_entry(L, l, ix, iy + 1));
+    const float2 t11 = __ldg(table + corner_entry(L, l, ix + 1, iy + 1));
+    const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
+    feat[size_t(2 * l) * N + n] = fmaf(w11, t11.x, fmaf(w01, t01.x, fmaf(w10, t10.x, w00 * t00.x)));
+    feat[size_t(2 * l + 1) * N + n] = fmaf(w11, t11.y, fmaf(w01, t01.y, fmaf(w10, t10.y, w00 * t00.y)));
+  }
+}
+
 // contributions: for coordinate n, level l, corner k -> key = entry,
 // item = n * levels + l (feature pair index), weight
 __global__ void __launch_bounds__(256) k_hash_contrib(const float2* __restrict__ coords, int N, const LevelTable L,
@@ -701,9 +727,14 @@ int ptycho_hashgrid_forward_planar(const float* coords, int N, const float* tabl
   if (!pty_aligned(coords, 8) || !pty_aligned(table, 8) || !pty_aligned(features_planar, 4))
     return PTYCHO_ERR_MISALIGNED;
   if (N == 0) return PTYCHO_OK;
+#ifndef PTY_HASH_FWD_PER_LEVEL
+  k_hash_fwd_planar_all<<<(unsigned)((N + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      reinterpret_cast<const float2*>(coords), N, reinterpret_cast<const float2*>(table), L, features_planar);
+#else
   const dim3 grid((unsigned)((N + 255) / 256), (unsigned)L.levels);
   k_hash_fwd_planar<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<const float2*>(coords), N, reinterpret_cast<const float2*>(table), L, features_planar);
+#endif
   return cudaGetLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_LAUNCH;
 }
 

@@ -115,10 +115,14 @@ int ptycho_forward_intensity_ws(const float* O, int H, int W, const float* P, in
  * added to instead of overwritten.  workspace: device scratch of at least
  * ptycho_fwd_adj_workspace_size() bytes, 256-byte aligned.  Imeas must be
  * 16-byte aligned (each pattern's measurement is fetched by a bulk copy).
- * Probes: M == N in {64, 128, 256} run the fused kernels; any other
- * 1 <= M, N <= 4096 (non-square, odd, 96, 192, ...) runs the general path:
- * the same losses and gradients through workspace passes (gather, row and
- * column DFTs of any length, loss, inverse DFTs), then the same assembly.
+ * Probes: M == N in {64, 128} run the fused kernels; M == N == 256 runs
+ * three line-DFT kernels over the workspace (smooth-L1, Poisson and the
+ * intensity-gradient code; batches of 192 or more also take dP from the
+ * inverse-row kernel) or, for the FD loss, one 4-CTA cluster per pattern;
+ * any other 1 <= M, N <= 4096 (non-square, odd, 96, 192, ...) runs the
+ * general path: the same losses and gradients through workspace passes
+ * (gather, row and column DFTs of any length, loss, inverse DFTs), then the
+ * same assembly.
  * ---------------------------------------------------------------------- */
 size_t ptycho_fwd_adj_workspace_size(int H, int W, int M, int N, int B);
 
