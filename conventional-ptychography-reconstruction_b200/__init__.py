@@ -6,7 +6,7 @@ The directory name is not a Python identifier; import it with
 ``importlib.import_module("conventional-ptychography-reconstruction_b200")``.
 """
 from . import _lib, optics, synth
-from . import accuracy, adam, cmlp, complex_inr, gsplat, hashgrid, probe_prep, resample, scan_shards
+from . import accuracy, adam, cmlp, complex_inr, gsplat, h5mat, hashgrid, probe_prep, resample, scan_shards
 from ._lib import PtychoError
 from .adam import FusedAdam
 from .complex_inr import ComplexINRModel2D

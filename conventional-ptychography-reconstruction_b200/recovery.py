@@ -35,7 +35,7 @@ import numpy as np
 import torch
 import yaml
 
-from . import optics, probe_prep, scan_shards
+from . import h5mat, optics, probe_prep, scan_shards
 from .adam import FusedAdam
 from .complex_inr import ComplexINRModel2D
 
@@ -74,12 +74,29 @@ def load_config(path):
 
 def load_ptychography_data(data_dir, bundle_file=None, location_file=None, raw_file=None, probe_file=None,
                            gt_file=None, init_probe_file=None, gap=1):
-    """.mat bundle or per-variable files -> dict (utils/io.py:72-122).  MATLAB
-    v7.3 (HDF5) files need h5py, which this environment does not provide."""
+    """.mat bundle or per-variable files -> dict (utils/io.py:72-122).  Files
+    are read as utils/io.py:read_data does: scipy's loadmat (v4 - v7), and
+    MATLAB v7.3 (HDF5) files through h5mat.read_mat73 (arrays transposed back
+    to MATLAB's dimension order, {real, imag} compounds made complex)."""
+    return _load(data_dir, bundle_file, location_file, raw_file, probe_file, gt_file, init_probe_file, gap)
+
+
+def read_data(file_path, key_name=None):
+    """One .mat file -> {name: value} (utils/io.py:25-69): loadmat first, the
+    v7.3 (HDF5) reader when loadmat cannot read the file."""
     from scipy.io import loadmat
 
+    try:
+        return loadmat(file_path)
+    except Exception:
+        if not h5mat.is_hdf5(file_path):
+            raise
+    return h5mat.read_mat73(file_path, key_name)
+
+
+def _load(data_dir, bundle_file, location_file, raw_file, probe_file, gt_file, init_probe_file, gap):
     def read(name):
-        return loadmat(os.path.join(data_dir, name))
+        return read_data(os.path.join(data_dir, name))
 
     out = {}
     if bundle_file is not None:
