@@ -471,13 +471,14 @@ __global__ void __launch_bounds__(256) k_gsep_rows(const GridArgs g) {
   const int k = sep_slot(g, g.sep_rb, b);
   const int l = g.sep_l[k], G = g.sep_gr[k];
   const int t = threadIdx.x, gl = t & (G - 1);
-  const long long item = ((b - g.sep_rb[k]) * 256 + t) / G;
-  const int E0 = g.E0[l];
-  const bool in = item < (long long)g.A * E0;
+  // 32-bit index math (A * E0 < 2^31; G is a power of two)
+  const unsigned item = unsigned(int(b - g.sep_rb[k]) * 256 + t) >> (__ffs(G) - 1);
+  const unsigned E0 = unsigned(g.E0[l]);
+  const bool in = item < unsigned(g.A) * E0;
   float s0x = 0.f, s0y = 0.f, s1x = 0.f, s1y = 0.f;
   if (in) {
     const int i = int(item / E0);
-    const int c = int(item - (long long)i * E0);
+    const int c = int(item - unsigned(i) * E0);
     const int* lo0 = g.lo0 + g.lo0off[l];
     const int j0 = lo0[c], j1 = lo0[c + 1];
     const float* fx0 = g.fx0 + size_t(l) * g.Bj;
@@ -519,13 +520,13 @@ __global__ void __launch_bounds__(256) k_gsep_cols(const GridArgs g) {
   const int k = sep_slot(g, g.sep_cb, b);
   const int l = g.sep_l[k], G = g.sep_gc[k];
   const int t = threadIdx.x, gl = t & (G - 1);
-  const long long item = ((b - g.sep_cb[k]) * 256 + t) / G;
+  const unsigned item = unsigned(int(b - g.sep_cb[k]) * 256 + t) >> (__ffs(G) - 1);
   const int E0 = g.E0[l], E1 = g.E1[l];
-  const bool in = item < (long long)E0 * E1;
+  const bool in = item < unsigned(E0) * unsigned(E1);
   const float4* H = g.H + g.sep_h[k];
   float ax = 0.f, ay = 0.f;
   if (in) {
-    const int cy = int(item / E0), cx = int(item - (long long)cy * E0);
+    const int cy = int(item / unsigned(E0)), cx = int(item - unsigned(cy) * unsigned(E0));
     auto Hat = [&](int i) {  // H[i][cx] = S1[i][cx - 1] + S0[i][cx]
       const float4 a0 = H[size_t(i) * E0 + cx];
       float2 h = make_float2(a0.x, a0.y);
@@ -622,6 +623,8 @@ __global__ void __launch_bounds__(256) k_gvert_tile(const GridArgs g) {
   __syncthreads();
   const int cx = cx0 + (t % kTX), cy = cy0 + (t / kTX);
   if (cx >= E0 || cy >= E1) return;
+  // (splitting each row's sum at lo0[cx] into two loops without the cell test
+  // measured slower on c4: 219 against 181 us)
   const int j0 = lo0[max(cx - 1, 0)] - j_lo, j1 = lo0[cx + 1] - j_lo;
   const int i0 = lo1[max(cy - 1, 0)] - i_lo, i1 = lo1[cy + 1] - i_lo;
   float ax = 0.f, ay = 0.f;
