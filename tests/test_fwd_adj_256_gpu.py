@@ -185,3 +185,58 @@ def test_intensity_gradient_256(pkg):
     dO, dP = _intensity_grad_ref(O, P, tlY, tlX, gI.astype(np.float64))
     assert rel_max(Ot.grad.cpu().numpy(), dO) <= 2e-4, rel_max(Ot.grad.cpu().numpy(), dO)
     assert rel_max(Pt.grad.cpu().numpy(), dP) <= 2e-4, rel_max(Pt.grad.cpu().numpy(), dP)
+
+
+def test_one_gradient_output_on_large_batches_256(pkg):
+    """B >= 192 takes dP from the inverse-row kernel: asking for dP alone or dO
+    alone gives bitwise what the call with both outputs gives."""
+    dev = torch.device("cuda")
+    B = 200
+    O, P, tlY, tlX, Imeas = _case(M, 420, B, seed=41)
+    Ot, Pt = torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev)
+    tl = pkg.make_windows(tlY, tlX, dev)
+    Im = torch.from_numpy(Imeas).to(dev)
+    code = pkg.LOSS_CODES["smooth_L1_loss"]
+    L = pkg.lib()
+    H = W = 420
+    ws_n = int(L.ptycho_fwd_adj_workspace_size(H, W, M, M, B))
+    st = pkg.optics.device_status(dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def call(want_o, want_p):
+        ws = torch.empty(ws_n, dtype=torch.uint8, device=dev)
+        loss = torch.zeros((), dtype=torch.float64, device=dev)
+        dO = torch.full((H, W), float("nan"), dtype=torch.complex64, device=dev) if want_o else None
+        dP = torch.full((M, M), float("nan"), dtype=torch.complex64, device=dev) if want_p else None
+        rc = L.ptycho_fwd_adj(Ot.data_ptr(), H, W, Pt.data_ptr(), M, M, tl.data_ptr(), Im.data_ptr(), B, None, B,
+                              code, None, loss.data_ptr(), dO.data_ptr() if want_o else None,
+                              dP.data_ptr() if want_p else None, 0, ws.data_ptr(), ws_n, st.data_ptr(), stream)
+        assert rc == 0, L.ptycho_status_string(rc)
+        torch.cuda.synchronize()
+        return float(loss), (dO.cpu().numpy() if want_o else None), (dP.cpu().numpy() if want_p else None)
+
+    l_both, dO_both, dP_both = call(True, True)
+    l_p, _, dP_only = call(False, True)
+    l_o, dO_only, _ = call(True, False)
+    assert l_both == l_p == l_o
+    assert np.array_equal(dP_only, dP_both) and np.array_equal(dO_only, dO_both)
+    r = fm.fwd_adj(O, P, tlY, tlX, Imeas, "smooth_L1_loss")
+    assert rel_max(dP_both, r["dP"]) <= 2e-4 and rel_max(dO_both, r["dO"]) <= 2e-4
+
+
+def test_loss_only_over_two_chunks_256(pkg):
+    """The loss-only mode (no gradient outputs) over 600 patterns (chunks of
+    512 and 88) against the FP64 oracle, pattern by pattern."""
+    dev = torch.device("cuda")
+    F = 50
+    O, P, tlY, tlX, Imeas = _case(M, 360, F, seed=43)
+    ids = np.random.default_rng(5).integers(0, F, 600).astype(np.int32)
+    loss, lp, _, _ = pkg.fwd_adj_raw(torch.from_numpy(O).to(dev), torch.from_numpy(P).to(dev),
+                                     pkg.make_windows(tlY, tlX, dev), torch.from_numpy(Imeas).to(dev),
+                                     pkg.LOSS_CODES["Poisson_likelihood_loss"], batch=torch.from_numpy(ids).to(dev),
+                                     want_grad=False, per_pattern=True)
+    lp = lp.cpu().numpy()
+    r = fm.fwd_adj(O, P, tlY, tlX, Imeas, "Poisson_likelihood_loss")  # each frame once
+    want = r["loss"][ids]
+    assert np.all(np.abs(lp - want) <= 2e-5 * np.abs(want))
+    assert abs(float(loss) - want.sum()) <= 2e-5 * abs(want.sum())
