@@ -7,7 +7,8 @@ built, loads, binds to the library and exports its entry points.  On the GPU:
 both routes give bit-identical losses and gradients (one library, one
 kernel sequence), for every loss, with one or both inputs requiring a
 gradient, a retained graph backed up twice, frame-id batches given as a list,
-and no-grad calls; argument errors raise the Python route's exception types.
+and no-grad calls; non-contiguous object / probe views and a side stream give
+the same values; argument errors raise the Python route's exception types.
 """
 import numpy as np
 import pytest
@@ -134,3 +135,46 @@ def test_cpp_node_no_grad_and_errors():
         pkg.fused_loss(Ot, Pt.to(torch.complex128), tl, Im, "smooth_L1_loss")
     with pytest.raises(ValueError):
         pkg.fused_loss(Ot, torch.zeros((4097, 4), dtype=torch.complex64, device=dev), tl, Im, "smooth_L1_loss")
+
+
+@pytest.mark.gpu
+def test_cpp_node_views_streams_and_id_types():
+    """Non-contiguous object / probe views give the contiguous copies' results
+    (gradients shaped like the views); a side stream gets its own workspace and
+    the same values; frame ids given as a NumPy array, int64 or on the host."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    pkg = load_pkg()
+    dev = torch.device("cuda")
+    O, P, tlY, tlX, Imeas = _case(128, 300, 10, seed=9)
+    tl = pkg.make_windows(tlY, tlX, dev)
+    Im = torch.from_numpy(Imeas).to(dev)
+    ids = np.array([3, 1, 4, 1, 5, 9], dtype=np.int64)
+
+    def run(Ot, Pt, batch, stream=None):
+        with torch.cuda.stream(stream) if stream is not None else torch.cuda.stream(torch.cuda.current_stream()):
+            loss = pkg.fused_loss(Ot, Pt, tl, Im, "Poisson_likelihood_loss", batch=batch)
+            loss.backward()
+        torch.cuda.synchronize()
+        return float(loss.detach()), Ot.grad.cpu().numpy(), Pt.grad.cpu().numpy()
+
+    base_O = torch.from_numpy(O).to(dev).requires_grad_(True)
+    base_P = torch.from_numpy(P).to(dev).requires_grad_(True)
+    ref = run(base_O, base_P, torch.from_numpy(ids.astype(np.int32)).to(dev))
+
+    # views: every other column of a wider buffer, and a transposed-then-transposed probe
+    wide = torch.zeros((300, 600), dtype=torch.complex64, device=dev)
+    wide[:, ::2] = torch.from_numpy(O).to(dev)
+    Ov = wide[:, ::2].detach().requires_grad_(True)
+    assert not Ov.is_contiguous()
+    Pv = torch.from_numpy(P.T.copy()).to(dev).t().detach().requires_grad_(True)
+    assert not Pv.is_contiguous()
+    got = run(Ov, Pv, ids)  # ids as a NumPy int64 array
+    assert got[0] == ref[0] and np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
+    assert Ov.grad.shape == Ov.shape and Pv.grad.shape == Pv.shape
+
+    side = torch.cuda.Stream()
+    O2 = torch.from_numpy(O).to(dev).requires_grad_(True)
+    P2 = torch.from_numpy(P).to(dev).requires_grad_(True)
+    got = run(O2, P2, torch.from_numpy(ids), stream=side)  # int64 on the host
+    assert got[0] == ref[0] and np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
