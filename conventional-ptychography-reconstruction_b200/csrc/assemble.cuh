@@ -4,7 +4,7 @@
 
 namespace pty {
 
-constexpr int kTile = 32;   // canvas tile edge for dO
+constexpr int kTile = 32;   // canvas tile height for dO (its width: 32 or 64, by window width)
 constexpr int kGroup = 16;  // patterns per dP partial sum
 constexpr int kPixBlock = 256;  // probe pixels per dP block
 
