@@ -54,9 +54,16 @@ T* fptr(const Tensor& t) {
 std::mutex g_ws_mu;
 std::unordered_map<uint64_t, Tensor> g_ws;
 
+// At most kMaxWorkspaces entries: a caller that keeps creating streams would
+// otherwise keep every old stream's workspace alive.  Dropping an entry is
+// safe: each workspace was allocated on its own stream, and the caching
+// allocator reuses freed memory in that stream's order.
+constexpr size_t kMaxWorkspaces = 16;
+
 Tensor workspace_on(const Tensor& like, cudaStream_t s, size_t bytes) {
   const uint64_t key = (uint64_t(like.device().index()) << 56) ^ reinterpret_cast<uintptr_t>(s);
   std::lock_guard<std::mutex> lock(g_ws_mu);
+  if (g_ws.size() >= kMaxWorkspaces && g_ws.find(key) == g_ws.end()) g_ws.clear();
   Tensor& w = g_ws[key];
   if (!w.defined() || size_t(w.numel()) < bytes)
     w = torch::empty({int64_t(bytes < 256 ? 256 : bytes)}, like.options().dtype(torch::kUInt8));

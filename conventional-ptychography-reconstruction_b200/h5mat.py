@@ -25,6 +25,7 @@ NotImplementedError with what was found.
 """
 from __future__ import annotations
 
+import mmap
 import struct
 import zlib
 
@@ -177,8 +178,14 @@ class _File:
             raise H5Error("bad local heap")
         return self.at(self.addr(h + 8 + 2 * self.sl))
 
+    def _nul(self, off: int) -> int:
+        end = self.d.find(b"\x00", off)
+        if end < 0:
+            raise H5Error(f"unterminated string at {off}")
+        return end
+
     def _cstr(self, off: int) -> str:
-        end = self.d.index(b"\x00", off)
+        end = self._nul(off)
         return self.d[off:end].decode("utf-8", "replace")
 
     def _symbol_table(self, btree: int, heap: int):
@@ -255,7 +262,7 @@ class _File:
             nmemb = bits & 0xFFFF
             names, formats, offsets = [], [], []
             for _ in range(nmemb):
-                end = self.d.index(b"\x00", p)
+                end = self._nul(p)
                 name = self.d[p:end].decode("ascii", "replace")
                 if ver < 3:
                     p += ((end - p) // 8 + 1) * 8  # null-terminated, padded to 8
@@ -483,12 +490,17 @@ def is_hdf5(path: str) -> bool:
 
 
 def read_mat73(path: str, key: str | None = None) -> dict:
-    """Variables of a MATLAB v7.3 file (utils/io.py:read_data, h5py branch)."""
+    """Variables of a MATLAB v7.3 file (utils/io.py:read_data, h5py branch).
+    The file is memory-mapped: only the pages of the objects read are loaded."""
     with open(path, "rb") as fh:
-        f = _File(fh.read())
-    top = f.children(f.root)
-    if top is None:
-        raise H5Error("the root object is not a group")
-    if key and key in top:
-        return {key: _convert(f, top[key])}
-    return {k: _convert(f, v) for k, v in top.items() if not k.startswith("#")}
+        size = fh.seek(0, 2)
+        if size == 0:
+            raise H5Error("empty file")
+        with mmap.mmap(fh.fileno(), 0, access=mmap.ACCESS_READ) as mm:
+            f = _File(mm)
+            top = f.children(f.root)
+            if top is None:
+                raise H5Error("the root object is not a group")
+            if key and key in top:
+                return {key: _convert(f, top[key])}
+            return {k: _convert(f, v) for k, v in top.items() if not k.startswith("#")}

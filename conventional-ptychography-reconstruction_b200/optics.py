@@ -245,6 +245,8 @@ def fwd_adj_raw(O, P, tl, Imeas, loss_code: int, batch=None, want_grad: bool = T
         # ordered, calls on different streams must not share scratch
         workspace = _default_ws.get((dev, stream))
         if workspace is None:
+            if len(_default_ws) >= 16:  # a caller creating streams would keep every old workspace
+                _default_ws.clear()
             workspace = _default_ws.setdefault((dev, stream), FwdAdjWorkspace())
         ws = workspace.get(ws_bytes, dev)
     st = device_status(dev)
