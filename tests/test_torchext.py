@@ -178,3 +178,26 @@ def test_cpp_node_views_streams_and_id_types():
     P2 = torch.from_numpy(P).to(dev).requires_grad_(True)
     got = run(O2, P2, torch.from_numpy(ids), stream=side)  # int64 on the host
     assert got[0] == ref[0] and np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
+
+
+@pytest.mark.gpu
+def test_cpp_node_many_streams():
+    """More streams than the workspace cache holds (16): entries are dropped,
+    results stay the same on every stream."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    pkg = load_pkg()
+    dev = torch.device("cuda")
+    O, P, tlY, tlX, Imeas = _case(64, 120, 6, seed=12)
+    tl = pkg.make_windows(tlY, tlX, dev)
+    Im = torch.from_numpy(Imeas).to(dev)
+    Ot = torch.from_numpy(O).to(dev)
+    Pt = torch.from_numpy(P).to(dev)
+    want = float(pkg.fused_loss(Ot, Pt, tl, Im, "smooth_L1_loss"))
+    streams = [torch.cuda.Stream() for _ in range(20)]
+    got = []
+    for st in streams:
+        with torch.cuda.stream(st):
+            got.append(pkg.fused_loss(Ot, Pt, tl, Im, "smooth_L1_loss"))
+    torch.cuda.synchronize()
+    assert all(float(g) == want for g in got)
